@@ -549,12 +549,17 @@ void orc_particle_particle_forces(const orc_int_params* ip, const orc_flp_params
   const int np = ip->NumParticles;
   const float rp = fp->ParticleDiam / 2.0f;
   const float W[3] = {(float)ip->SystemSize[0], (float)ip->SystemSize[1], (float)ip->SystemSize[2]};
+  const int nzones = ip->NumZones[0] * ip->NumZones[1] * ip->NumZones[2];
   for (int th = 0; th < numParThreads; th++)
     for (int i = 0; i < numParInThread[th]; i++) {
       int pi = threadMembers[th * np + i];
       int pz = parsZone[pi];
       for (int nz = 1; nz <= zoneNeighDat[pz * 28]; nz++) {
         int zid = zoneNeighDat[pz * 28 + nz];
+        /* The y-stride quirk of D3Q19-OpenCL.c:450 can name zones past the
+         * end of the zone arrays when NumZones[2] > NumZones[1]; the
+         * reference then reads out of bounds.  Such zones count as empty. */
+        if (zid < 0 || zid >= nzones) continue;
         for (int j = 0; j < numParInZone[zid]; j++) {
           int pj = zoneMembers[zid * np + j];
           if (!(pi > pj)) continue;
