@@ -1,0 +1,384 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 D3Q19 LBM + IBM time step.
+
+Workload (default "dense-powerlaw-128"): the dense power-law suspension --
+128^3 lattice (126^3 interior nodes, z walls at +-0.05 lu/step, periodic x/y),
+200 freely moving spheres of diameter 16 with 512 IBM markers each placed by
+seeded random sequential addition with a 2 lu minimum gap (phi = 21.6 %),
+power-law fluid n = 0.6, k = 0.0105, local tau clamped to [0.55, 2.0].  A
+step is one full time step (collide-stream with boundaries, IBM, rigid
+bodies, particle contacts, zone rebuild every 10 steps).
+
+Metric: MLUPS = interior nodes x steps / s / 1e6, summed over GPUs (each GPU
+runs an independent replica: weak scaling, no collective on the data path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "dispersion-shear_d3q19-opencl_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, REPO)
+
+BYTES_PER_NODE = 152  # 19 populations read + 19 written, FP32
+
+WORKLOADS = {
+    "dense-powerlaw-128": dict(
+        iterations=10000, total_lattice_size=(128, 128, 128), boundary_conditions_xyz=(0, 0, 1), newtonian_tau=1.0,
+        viscosity_model=2, viscosity_params=(0.0105, 0.6, 0.0, 0.0), use_constant_viscosity=0, tau_min=0.55,
+        tau_max=2.0, velocity_bc_upper=(0.05, 0.0, 0.0), velocity_bc_lower=(-0.05, 0.0, 0.0), initial_f="constant",
+        initial_vel=(0.0, 0.0, 0.0), num_particles=200, particle_diameter=16.0, ibm_points_per_particle=512,
+        initial_particle_distribution=4, particle_seed=1, min_particle_gap=2.0, initial_particle_buffer=0.0,
+        z_wall_particle_buffer=9.0, domain_decomposition=(1, 1, 1), rebuild_neigh_list_freq=10,
+        particle_collision_params=2.0, video_freq=1000000, shear_stress_freq=1000000, console_print_freq=1000000),
+}
+DESCRIPTION = {
+    "dense-powerlaw-128": "dense power-law suspension: 128^3 lattice, 200 spheres d=16 (512 markers, RSA seed 1, "
+                          "gap 2), n=0.6 k=0.0105 tau in [0.55,2], walls +-0.05",
+}
+
+# The same workload as the reference host can express it: its marker rule
+# (1024 points for d=16), jittered-grid placement (distribution 2) instead of
+# seeded RSA, no tau clamps, the build without USE_CONSTANT_VISCOSITY.
+REFERENCE_KEYWORDS = {
+    "dense-powerlaw-128": dict(
+        total_lattice_size=(128, 128, 128), boundary_conditions_xyz=(0, 0, 1), newtonian_tau=1.0,
+        viscosity_model=2, viscosity_params=(0.0105, 0.6, 0.0, 0.0), velocity_bc_upper=(0.05, 0.0, 0.0),
+        velocity_bc_lower=(-0.05, 0.0, 0.0), initial_f="constant", initial_vel=(0.0, 0.0, 0.0), num_particles=200,
+        particle_diameter=16.0, initial_particle_distribution=2, random_particle_shift=0.0,
+        initial_particle_buffer=8.0, z_wall_particle_buffer=2.0, domain_decomposition=(1, 1, 1),
+        rebuild_neigh_list_freq=10, particle_collision_params=2.0, video_freq=1000000, shear_stress_freq=1000000,
+        console_print_freq=1000000),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed
+    region (the GPU's physical index resolved through CUDA_VISIBLE_DEVICES)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        self.index = str(local_rank)
+        if vis:
+            ids = [v.strip() for v in vis.split(",") if v.strip()]
+            if local_rank < len(ids):
+                self.index = ids[local_rank]
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.index, "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+def measured_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(workload):
+    """DRAM bytes per launch of the collide-stream kernel from the committed
+    ncu summary (profiles/), or None."""
+    p = os.path.join(REPO, "profiles", f"fluid_step_kernel_{workload}.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return d.get("dram_bytes_per_launch_full_size")
+    except (OSError, ValueError):
+        return None
+
+
+def setup(workload, device):
+    import numpy as np  # noqa: F401
+
+    import d3q19_b200 as d3
+
+    cfg = d3.parse_config(d3.keywords_text(WORKLOADS[workload]))
+    hs = d3.HostState(cfg, data_dir=os.getcwd())
+    hs.options.device = device
+    sim = d3.Simulation.from_host_state(hs, device=device)
+    return d3, hs, sim
+
+
+def launches(ip, rebuild, t0, k):
+    n = 0
+    for t in range(t0, t0 + k):
+        n += 1
+        if ip.NumParticles > 0:
+            n += 1 + (1 if t % rebuild == 0 else 0)
+    return n
+
+
+def run_ours(args, rank, world, local_rank, dist):
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    d3, hs, sim = setup(args.workload, local_rank)
+    ip = hs.cfg.ip
+    interior = (ip.LatticeSize[0] - 2) * (ip.LatticeSize[1] - 2) * (ip.LatticeSize[2] - 2)
+    R = hs.cfg.hp.RebuildFreq
+    stream = torch.cuda.ExternalStream(sim.stream_ptr, device=local_rank)
+    t = 1
+    sim.run(t, args.warmup)
+    t += args.warmup
+    sim.synchronize()
+
+    # Timed region: exactly K steps, barrier + synchronize on both sides.
+    clocks = ClockSampler(local_rank)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(t, args.steps)
+    e1.record(stream)
+    sim.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    t += args.steps
+    n_launch = launches(ip, R, t - args.steps, args.steps)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+
+    # Per-launch device time of the collide-stream kernel (events around
+    # each launch on the library's stream), for the roofline.
+    kp = min(args.steps, 200)
+    sim.profile(True)
+    sim.run(t, kp)
+    fluid_ms, nf, part_ms, npart = sim.profile_read()
+    sim.profile(False)
+    t += kp
+    fluid_avg = fluid_ms / max(nf, 1)
+    part_avg = part_ms / max(npart, 1)
+
+    # End to end through the C ABI: pinned host buffers uploaded, K steps,
+    # velocity and particle state read back.
+    def pinned(a):
+        buf = torch.empty(a.size, dtype=torch.float32 if a.dtype.kind == "f" else torch.int32, pin_memory=True)
+        out = buf.numpy()
+        out[:] = a
+        return out
+
+    hf, hu, htau = pinned(hs.f), pinned(hs.u), pinned(hs.tau)
+    hk, hpf, hpff, hsp = pinned(hs.parKin), pinned(hs.parForce), pinned(hs.parFluidForce), pinned(hs.spherePoints)
+    ru, rk, rpff = pinned(np.zeros(3 * sim.nc, np.float32)), pinned(np.zeros(max(hs.parKin.size, 1), np.float32)), \
+        pinned(np.zeros(max(hs.parFluidForce.size, 1), np.float32))
+    sim2 = d3.Simulation(hs.cfg.ip, hs.cfg.fp, hs.options)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    sim2.write_lattice(hf, hu, htau)
+    sim2.write_periodic_map(d3.periodic_map(hs.cfg.ip))
+    if sim2.np > 0:
+        sim2.write_particles(hk, hpf, hpff, hsp)
+        sim2.write_zones(hs.zoneNeighDat, hs.parsZone, hs.zoneMembers, hs.numParInZone, hs.threadMembers,
+                         hs.numParInThread)
+    sim2.run(1, args.steps)
+    ru[:] = sim2.read_u()
+    if sim2.np > 0:
+        rk[:] = sim2.read_parkin()
+        rpff[:] = sim2.read_parfluidforce()
+    e2e_s = time.perf_counter() - w0
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_s = float(e2e_t.item())
+    h2d = hf.nbytes + hu.nbytes + htau.nbytes + hk.nbytes + hpf.nbytes + hpff.nbytes + hsp.nbytes
+    d2h = ru.nbytes + (rk.nbytes + rpff.nbytes if sim2.np > 0 else 0)
+    sim2.close()
+    sim.close()
+
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_NODE * interior / (fluid_avg * 1e-3) / 1e9
+    value = world * interior * args.steps / (ms_max * 1e-3) / 1e6
+    out = {
+        "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded RSA placement)",
+        "impl": "ours",
+        "config": {"workload": args.workload, "description": DESCRIPTION[args.workload],
+                   "lattice": list(ip.LatticeSize), "interior_nodes": interior, "spheres": ip.NumParticles,
+                   "markers_per_sphere": ip.PointsPerParticle, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (2 x 19 x 4 B x 2.1 M nodes = 320 MB distributions)"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": ncu_traffic(args.workload),
+                     "kernel": "fluid_step_kernel", "bytes_per_node": BYTES_PER_NODE,
+                     "kernel_ms": round(fluid_avg, 5), "particle_kernel_ms": round(part_avg, 5),
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+                     "fallback 6.65 TB/s",
+                     "step_frac": round(value / world * 1e6 * BYTES_PER_NODE / 1e9 / peak, 4)},
+        "e2e": {"value": round(world * interior * args.steps / e2e_s / 1e6, 1), "unit": "MLUPS",
+                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+                "note": "C-ABI calls from pinned host buffers: upload of the initial state, K steps, read-back "
+                        "of u, sphere kinematics and forces"},
+        "gpu_launches": n_launch,
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args.workload)
+    return out
+
+
+# ---------------------------------------------------------------------------
+def _reference_run(workload, iters, threads):
+    """Wall time of the reference's own program (built from its sources for
+    the host cores, oracle/_ref) for `iters` steps of the workload."""
+    from oracle import pyoracle as po
+
+    kw = dict(REFERENCE_KEYWORDS[workload], iterations=iters)
+    t0 = time.perf_counter()
+    po.run_reference(kw, variable_viscosity=True, serial=False, dump=False, threads=threads,
+                     workdir=tempfile.mkdtemp(prefix="d3q19bench_"))
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(workload, sample_steps=8):
+    """CPU throughput of the reference on the box's host cores: the difference
+    of two runs (1 and 1 + sample_steps steps) removes the set-up time."""
+    from oracle import pyoracle as po
+
+    threads = os.cpu_count() or 1
+    kw = WORKLOADS[workload]
+    N = kw["total_lattice_size"]
+    interior = (N[0] - 2) * (N[1] - 2) * (N[2] - 2)
+    if po.ref_available():
+        ta = _reference_run(workload, 1, threads)
+        tb = _reference_run(workload, 1 + sample_steps, threads)
+        per = max(tb - ta, 1e-9) / sample_steps
+        return {"value": round(interior / per / 1e6, 3), "unit": "MLUPS", "cores": threads, "kind": "reference",
+                "sample": f"{sample_steps} steps of the reference's own program (GPU_program.cl without "
+                          "USE_CONSTANT_VISCOSITY + CPU_program.cl + D3Q19-OpenCL.c, mock OpenCL runtime, "
+                          f"{threads} OpenMP threads) on the 128^3 lattice with 200 d=16 spheres; per-step time from "
+                          "the difference of a 1-step and a 9-step run; reference marker rule (1024/sphere) and "
+                          "jittered-grid placement"}
+    return {"value": None, "unit": "MLUPS", "cores": threads, "kind": "reference",
+            "sample": "oracle/_ref not built on this machine"}
+
+
+def run_reference_arm(args):
+    b = cpu_baseline(args.workload, sample_steps=max(1, min(args.steps, 8)))
+    kw = WORKLOADS[args.workload]
+    N = kw["total_lattice_size"]
+    out = {"impl": "reference", "metric": "MLUPS", "value": b["value"], "unit": "MLUPS", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": (round((N[0] - 2) * (N[1] - 2) * (N[2] - 2) / (b["value"] * 1e6) * 1e3, 3)
+                           if b["value"] else None),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic", "config": {"workload": args.workload, "description": DESCRIPTION[args.workload]},
+           "cpu_baseline": b, "e2e": {"value": b["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}
+    if b["value"] is None:
+        out = {"impl": "reference", "unavailable": b["sample"]}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10000)
+    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dense-powerlaw-128", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference_arm(args)), flush=True)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    try:
+        out = run_ours(args, rank, world, local_rank, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

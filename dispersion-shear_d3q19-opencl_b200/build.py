@@ -1,0 +1,73 @@
+"""Build recipe of the native parts, in-tree:
+
+  lib/libd3q19_b200.so   CUDA kernels + C ABI (nvcc, sm_100a, static cudart)
+  lib/libd3q19_host.so   C host routines (parser, initial state, outputs)
+  bin/d3q19_b200         the simulation program (drop-in for the reference's binary)
+
+Usage: python build.py [--force]
+"""
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(PKG)
+LIB = os.path.join(PKG, "lib")
+BIN = os.path.join(PKG, "bin")
+CUDA_LIB = os.path.join(LIB, "libd3q19_b200.so")
+HOST_LIB = os.path.join(LIB, "libd3q19_host.so")
+MAIN = os.path.join(BIN, "d3q19_b200")
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CU_SRC = [os.path.join(PKG, "csrc", f) for f in ("d3q19_kernels.cu", "d3q19_api.cu", "d3q19_exact.cu")]
+# Translation units compiled without floating-point contraction: the
+# reference-exact arithmetic.
+NO_CONTRACT = {"d3q19_exact.cu"}
+OBJ = os.path.join(PKG, "_build")
+CU_HDR = [os.path.join(PKG, "csrc", "d3q19_internal.h"), os.path.join(REPO, "include", "d3q19_b200.h")]
+HOST_SRC = [os.path.join(PKG, "host", "d3q19_host.c")]
+HOST_HDR = [os.path.join(PKG, "host", "d3q19_host.h"), os.path.join(REPO, "include", "d3q19_b200.h")]
+MAIN_SRC = [os.path.join(PKG, "host", "d3q19_main.c")]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
+def build(force: bool = False, verbose_ptxas: bool = False):
+    os.makedirs(LIB, exist_ok=True)
+    os.makedirs(BIN, exist_ok=True)
+    if force or _stale(CUDA_LIB, CU_SRC + CU_HDR + [__file__]):
+        os.makedirs(OBJ, exist_ok=True)
+        objs = []
+        for src in CU_SRC:
+            obj = os.path.join(OBJ, os.path.basename(src) + ".o")
+            cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-c", "-o", obj, src]
+            if os.path.basename(src) in NO_CONTRACT:
+                cmd.insert(1, "--fmad=false")
+            if verbose_ptxas:
+                cmd.insert(1, "-Xptxas=-v")
+            _run(cmd)
+            objs.append(obj)
+        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", CUDA_LIB] + objs)
+    if force or _stale(HOST_LIB, HOST_SRC + HOST_HDR + [__file__]):
+        _run(["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-Wall", "-Wno-unused-result", "-o", HOST_LIB]
+             + HOST_SRC + ["-lm"])
+    if force or _stale(MAIN, MAIN_SRC + HOST_SRC + HOST_HDR + [CUDA_LIB, __file__]):
+        _run(["gcc", "-O2", "-std=gnu11", "-Wall", "-Wno-unused-result", "-o", MAIN] + MAIN_SRC + HOST_SRC
+             + ["-L" + LIB, "-ld3q19_b200", "-Wl,-rpath,$ORIGIN/../lib", "-lm", "-lstdc++", "-lpthread", "-ldl",
+                "-lrt"])
+    return CUDA_LIB, HOST_LIB, MAIN
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose_ptxas="-v" in sys.argv)

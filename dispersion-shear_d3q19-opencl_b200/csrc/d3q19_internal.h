@@ -1,0 +1,147 @@
+// d3q19_internal.h -- types shared by the kernels (d3q19_kernels.cu) and the
+// C-ABI layer (d3q19_api.cu).  Not part of the public interface.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace d3q19 {
+
+// Fluid tile handled by one thread block of the collide-stream kernel: a run
+// of 32 x-nodes (one warp) by TILE_Y rows by TILE_Z planes; the 256 threads
+// (32 x 4 x 2) take TILE_Z/2 planes each.  The IBM force of a tile is
+// accumulated over the tile plus a one-node halo.
+constexpr int TILE_X = 32;
+constexpr int TILE_Y = 4;
+constexpr int TILE_Z = 4;
+constexpr int FLUID_THREADS = TILE_X * TILE_Y * 2;
+constexpr int HALO_X = TILE_X + 2;
+constexpr int HALO_Y = TILE_Y + 2;
+constexpr int HALO_Z = TILE_Z + 2;
+constexpr int HALO_N = HALO_X * HALO_Y * HALO_Z;
+
+// The spread force is accumulated in fixed point (deterministic: integer sums
+// do not depend on the order markers are visited in).  A contribution v,
+// |v| < 2^FIX_BITS units of 2^-FIX_BITS times the largest marker force of the
+// step, is split as v = hi * 2^16 + lo (0 <= lo < 2^16) and the two parts are
+// summed with 32-bit atomics: exact for up to 2^(31 + 16 - FIX_BITS) = 256
+// contributions of the largest size per node.
+constexpr int FIX_BITS = 39;
+
+// Device error word bits.
+constexpr unsigned ERR_TILE_OVERFLOW = 1u;
+constexpr unsigned ERR_NONFINITE = 2u;
+constexpr unsigned ERR_ZONE_RANGE = 4u;
+constexpr unsigned ERR_FIXED_RANGE = 8u;
+
+struct Geom {
+  int Nx, Ny, Nz;
+  long long NC;    // Nx*Ny*Nz
+  int periodic[3]; // BoundaryConds == 0
+  int wallAxis;    // axis with BoundaryConds == 1, or -1
+  int tanBC[3];    // tangential velocity boundaries (only with a wall axis)
+  int buffer[3];   // BufferSize
+  int ntx, nty, ntz;  // fluid tiles per axis
+};
+
+struct FluidParams {
+  float g[3];           // ConstBodyForce
+  float tauN;           // NewtonianTau
+  float velLower[3], velUpper[3];
+  int viscModel;
+  float visc[4];
+  float tauMax;         // 0 = no upper clamp
+  float tauMin;         // lower clamp (the reference's MIN_TAU = 0.505)
+  float cassonReg;      // 0 = none
+};
+
+// One IBM marker of the last particle pass, two float4 per marker:
+//   a = {wx, wy, wz, bits(x0 | y0 << 16)}, b = {Fx, Fy, Fz, bits(z0)}
+// (x0, y0, z0) is the corner cell of the marker's 2x2x2 stencil including
+// the buffer offset, w* the reference's linear weights, F the marker force.
+struct TileLists {
+  int cap;
+  int* count;          // [ntiles]
+  int* list;           // [ntiles * cap] marker ids
+  const float4* mrec;  // [2 * markers]
+  unsigned* fmax;      // [2] float bits of the largest |marker force| per step parity
+};
+
+struct FluidArgs {
+  Geom g;
+  FluidParams p;
+  int t;  // time step (selects the marker-force maximum slot)
+  const float* fin;
+  float* fout;
+  float* u;
+  float* tau;
+  TileLists tiles;
+  int has_ibm;
+  unsigned* err;
+  unsigned long long* clamps;
+};
+
+struct ParticleParams {
+  int np, P, L, nfa;        // spheres, markers per sphere, work-group size, groups per sphere
+  float S[3];               // SystemSize as float
+  int Sint[3];
+  int buffer[3];
+  float mass, inertia, pointArea, diam, zbuf;
+  float g[3];
+  float kcol;               // ParForceParams[0]
+  int forceModel;           // ParForceModel
+  int viscModel;
+  float tauN;
+  int numZones[3];
+  float zoneWidth[3];
+  int fixed;
+  int exact;  // contact forces summed in the reference's order
+};
+
+struct ParticleArgs {
+  Geom g;
+  ParticleParams p;
+  // state at t-1 (read) and t (written)
+  const float4* kin_old;
+  float4* kin_new;
+  const float4* pff_old;   // parFluidForce partials of step t-1
+  float4* pff_new;
+  const float4* pf_old;    // parForce of step t-1
+  float4* pf_new;
+  const float4* sphere;    // spherePoints [P]
+  const float* u;
+  float4* mrec;
+  TileLists tiles;
+  const int* znd;          // zoneNeighDat [28*Z]
+  const int* parsZone;
+  const int* zoneMembers;
+  const int* numParInZone;
+  const int* revStart;     // reverse zone-neighbour table (CSR)
+  const int* revList;
+  unsigned* err;
+  int t;
+};
+
+struct ZoneArgs {
+  ParticleParams p;
+  const float4* kin;
+  int* parsZone;
+  int* zoneMembers;
+  int* numParInZone;
+  int* zoneOf;
+  unsigned* err;
+};
+
+// Launchers (d3q19_kernels.cu).
+cudaError_t launch_fluid(const FluidArgs& a, bool first, bool variable, int collision, cudaStream_t s);
+cudaError_t launch_materialize_f(const FluidArgs& a, float* out, cudaStream_t s);
+cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s);
+cudaError_t launch_zones(const ZoneArgs& a, cudaStream_t s);
+cudaError_t launch_spread_field(const Geom& g, const TileLists& t, int last_step, float* out, unsigned* err,
+                                cudaStream_t s);
+cudaError_t launch_marker_cells(const float4* mrec, int M, int* cells, cudaStream_t s);
+// Reference-exact variants (d3q19_exact.cu, compiled without contraction).
+cudaError_t launch_fluid_exact(const FluidArgs& a, bool first, bool variable, int slots, cudaStream_t s);
+cudaError_t launch_spread_field_exact(const Geom& g, const TileLists& t, int slots, float* out, unsigned* err,
+                                      cudaStream_t s);
+
+}  // namespace d3q19

@@ -1,0 +1,1029 @@
+// d3q19_kernels.cu -- sm_100a kernels of the D3Q19 LBM + IBM time step.
+//
+// Kernel map (reference kernel -> kernel here):
+//   collideMRT_stream_D3Q19 (GPU_program.cl:316-624)
+//   + boundary_periodic     (GPU_program.cl:626-735)
+//   + boundary_velocity     (GPU_program.cl:737-865)
+//   + reset/sum_particle_fluid_forces and the 27-point force smoothing
+//                           (GPU_program.cl:258-313, 356-377)
+//       -> fluid_step_kernel: one pass per node.  The reference pushes
+//          post-collision populations to the neighbours and then repairs the
+//          boundary layer with two more kernels.  Here each node pulls its
+//          populations from the neighbours' post-collision values, wrapping
+//          periodic axes and rebuilding the wall unknowns in registers, which
+//          yields exactly the reference's post-boundary state, then collides
+//          and stores its own post-collision values (aligned stores).  The
+//          IBM force of the previous step is accumulated per tile in shared
+//          memory from the markers listed for that tile (integer fixed-point
+//          sums: deterministic) and smoothed with the reference's 27-point
+//          stencil, so no dense force field ever touches HBM.
+//   particle_dynamics (CPU_program.cl:187-277)
+//   + particle_fluid_forces_linear_stencil (GPU_program.cl:81-256)
+//   + particle_particle_forces (CPU_program.cl:76-184)
+//       -> particle_step_kernel: one block per reference work-group of
+//          markers; each block advances its sphere (rigid-body update from
+//          the forces of step t-1), interpolates u(t) at its markers,
+//          reduces force and torque over the work-group in the reference's
+//          tree order, writes the marker records and lists each marker in
+//          the fluid tiles its stencil touches (bucket sort by tile).  Extra
+//          blocks compute the particle-particle forces, one thread per
+//          sphere, from the same updated positions.
+//   update_particle_zones (CPU_program.cl:280-315) -> zone_rebuild_kernel.
+#include "d3q19_internal.h"
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace d3q19 {
+
+// D3Q19 velocities in the reference's order (D3Q19-OpenCL.c:9-13), as
+// compile-time expressions of q so fully unrolled loops fold them.
+#define CXQ(q) (((q) == 1 || (q) == 7 || (q) == 8 || (q) == 9 || (q) == 10) ? 1 : \
+                (((q) == 2 || (q) == 11 || (q) == 12 || (q) == 13 || (q) == 14) ? -1 : 0))
+#define CYQ(q) (((q) == 3 || (q) == 7 || (q) == 11 || (q) == 15 || (q) == 16) ? 1 : \
+                (((q) == 4 || (q) == 8 || (q) == 12 || (q) == 17 || (q) == 18) ? -1 : 0))
+#define CZQ(q) (((q) == 5 || (q) == 9 || (q) == 13 || (q) == 15 || (q) == 17) ? 1 : \
+                (((q) == 6 || (q) == 10 || (q) == 14 || (q) == 16 || (q) == 18) ? -1 : 0))
+#define CAQ(A, q) ((A) == 0 ? CXQ(q) : ((A) == 1 ? CYQ(q) : CZQ(q)))
+// Opposite direction.
+#define OPPQ(q) ((q) == 0 ? 0 : (q) <= 6 ? (((q) & 1) ? (q) + 1 : (q) - 1) : \
+                 (q) == 7 ? 12 : (q) == 12 ? 7 : (q) == 8 ? 11 : (q) == 11 ? 8 : \
+                 (q) == 9 ? 14 : (q) == 14 ? 9 : (q) == 10 ? 13 : (q) == 13 ? 10 : \
+                 (q) == 15 ? 18 : (q) == 18 ? 15 : (q) == 16 ? 17 : 16)
+
+// ---------------------------------------------------------------------------
+// Wet-node velocity boundary (GPU_program.cl:737-865 with calcRho = 0, the
+// momentum correction off): on the wall plane of axis A (SIDE 0 = lower,
+// inward normal +A; SIDE 1 = upper), rho = 1, the inward normal velocity
+// follows from the knowns, and each unknown is its opposite population plus
+// rho*(u_n + c_t.u_t)/6, or rho*u_n/3 for the normal direction.
+template <int A, int SIDE>
+__device__ __forceinline__ void velocity_bc(float (&f)[19], const float* uw) {
+  constexpr int IN = SIDE == 0 ? 1 : -1;
+  constexpr int A1 = A == 0 ? 1 : 0;
+  constexpr int A2 = A == 2 ? 1 : 2;
+  float sum9 = 0.0f, sum5 = 0.0f;
+#pragma unroll
+  for (int q = 0; q < 19; q++) {
+    if (CAQ(A, q) == 0) sum9 += f[q];
+    else if (CAQ(A, q) == -IN) sum5 += f[q];
+  }
+  const float rho = 1.0f;
+  const float un = 1.0f - (sum9 + 2.0f * sum5) / rho;
+  const float ua1 = uw[A1], ua2 = uw[A2];
+#pragma unroll
+  for (int q = 1; q < 19; q++) {
+    if (CAQ(A, q) != IN) continue;
+    const int t1 = CAQ(A1, q), t2 = CAQ(A2, q);
+    float v;
+    if (t1 == 0 && t2 == 0) {
+      v = f[OPPQ(q)] + rho * un / 3.0f;
+    } else if (t1 != 0) {
+      v = f[OPPQ(q)] + rho * (t1 > 0 ? un + ua1 : un - ua1) / 6.0f;
+    } else {
+      v = f[OPPQ(q)] + rho * (t2 > 0 ? un + ua2 : un - ua2) / 6.0f;
+    }
+    f[q] = v;
+  }
+}
+
+__device__ __forceinline__ void apply_wall(float (&f)[19], int axis, int side, const FluidParams& p) {
+  const float* uw = side ? p.velUpper : p.velLower;
+  if (axis == 0) {
+    if (side) velocity_bc<0, 1>(f, uw); else velocity_bc<0, 0>(f, uw);
+  } else if (axis == 1) {
+    if (side) velocity_bc<1, 1>(f, uw); else velocity_bc<1, 0>(f, uw);
+  } else {
+    if (side) velocity_bc<2, 1>(f, uw); else velocity_bc<2, 0>(f, uw);
+  }
+}
+
+// Local relaxation time (GPU_program.cl:1041-1128).  Optional extensions:
+// an upper clamp and a regularised Casson yield term.
+__device__ __forceinline__ float compute_tau(const FluidParams& p, float srt, bool& clamped) {
+  float tau = p.tauN;
+  const float eps = 1e-8f;
+  if (p.viscModel == 2) {  // power law
+    float k = p.visc[0], n = p.visc[1], nu;
+    srt = srt > eps ? srt : eps;
+    if (n == 0.5f) nu = k / sqrtf(srt);
+    else if (n == 1.0f) nu = k;
+    else if (n == 2.0f) nu = k * srt;
+    else nu = k * powf(srt, n - 1.0f);
+    tau = 3.0f * nu + 0.5f;
+  } else if (p.viscModel == 4) {  // Casson
+    float tY = p.visc[0], eta = p.visc[1];
+    srt = srt > eps ? srt : eps;
+    float sr = p.cassonReg > 0.0f ? sqrtf(srt * srt + p.cassonReg * p.cassonReg) : srt;
+    float a = sqrtf(tY / sr) + sqrtf(eta);
+    tau = 3.0f * (a * a) + 0.5f;
+  } else if (p.viscModel == 3) {  // Herschel-Bulkley
+    float tY = p.visc[0], k = p.visc[1], n = p.visc[2], nu;
+    srt = srt > eps ? srt : eps;
+    if (n == 0.5f) nu = tY / srt + k / sqrtf(srt);
+    else if (n == 1.0f) nu = tY / srt + k;
+    else if (n == 2.0f) nu = tY / srt + k * srt;
+    else nu = tY / srt + k * powf(srt, n - 1.0f);
+    tau = 3.0f * nu + 0.5f;
+  } else {
+    return tau;
+  }
+  clamped = false;
+  if (p.tauMin > 0.0f) {
+    if (tau < p.tauMin) {
+      tau = p.tauMin;
+      clamped = true;
+    }
+  } else if ((double)tau < 0.505) {  // MIN_TAU is a double constant (GPU_program.cl:6)
+    tau = 0.505f;
+    clamped = true;
+  }
+  if (p.tauMax > 0.0f && tau > p.tauMax) tau = p.tauMax;
+  return tau;
+}
+
+// Populations pulled from the neighbours' post-collision values:
+// population q of node i comes from node i - c_q, wrapped on periodic axes.
+// On a wall plane the sources outside the lattice interior are the buffer
+// layer; those populations are unknowns and are rebuilt by velocity_bc.
+__device__ __forceinline__ void gather(float (&f)[19], const float* __restrict__ fin, long long NC, long long i,
+                                       int dxm, int dxp, int dym, int dyp, int dzm, int dzp) {
+#pragma unroll
+  for (int q = 0; q < 19; q++) {
+    const int cx = CXQ(q), cy = CYQ(q), cz = CZQ(q);
+    long long src = i + (cx == 1 ? dxm : (cx == -1 ? dxp : 0)) + (cy == 1 ? dym : (cy == -1 ? dyp : 0)) +
+                    (cz == 1 ? dzm : (cz == -1 ? dzp : 0));
+    f[q] = __ldg(fin + q * NC + src);
+  }
+}
+
+// Index deltas to the upwind neighbours of node (x,y,z).
+__device__ __forceinline__ void neighbour_deltas(const Geom& g, int x, int y, int z, int& dxm, int& dxp, int& dym,
+                                                 int& dyp, int& dzm, int& dzp) {
+  const int Nxy = g.Nx * g.Ny;
+  dxm = (g.periodic[0] && x == 1) ? g.Nx - 3 : -1;
+  dxp = (g.periodic[0] && x == g.Nx - 2) ? -(g.Nx - 3) : 1;
+  dym = ((g.periodic[1] && y == 1) ? g.Ny - 3 : -1) * g.Nx;
+  dyp = ((g.periodic[1] && y == g.Ny - 2) ? -(g.Ny - 3) : 1) * g.Nx;
+  dzm = ((g.periodic[2] && z == 1) ? g.Nz - 3 : -1) * Nxy;
+  dzp = ((g.periodic[2] && z == g.Nz - 2) ? -(g.Nz - 3) : 1) * Nxy;
+}
+
+// Boundary rebuild after the gather: the wall plane of the wall axis, then
+// the tangential velocity boundaries in axis order (sim_main.c:383-402).
+__device__ __forceinline__ void boundaries(float (&f)[19], const Geom& g, const FluidParams& p, int x, int y,
+                                           int z) {
+  if (g.wallAxis < 0) return;
+  const int c[3] = {x, y, z};
+  const int N[3] = {g.Nx, g.Ny, g.Nz};
+  const int a = g.wallAxis;
+  if (c[a] == 1) apply_wall(f, a, 0, p);
+  else if (c[a] == N[a] - 2) apply_wall(f, a, 1, p);
+#pragma unroll
+  for (int t = 0; t < 3; t++) {
+    if (!g.tanBC[t]) continue;
+    if (c[t] == 1) apply_wall(f, t, 0, p);
+    else if (c[t] == N[t] - 2) apply_wall(f, t, 1, p);
+  }
+}
+
+// Inverse squared norms of the moment basis rows (rho, e, eps, jx, qx, jy,
+// qy, jz, qz, 3pxx, 3pixx, pww, piww, pxy, pyz, pxz, mx, my, mz).
+#define INV_N1 (1.0f / 2394.0f)
+#define INV_N2 (1.0f / 252.0f)
+#define INV_N4 (1.0f / 40.0f)
+#define INV_N9 (1.0f / 36.0f)
+#define INV_N10 (1.0f / 72.0f)
+#define INV_N11 (1.0f / 12.0f)
+#define INV_N12 (1.0f / 24.0f)
+#define INV_N13 (1.0f / 4.0f)
+#define INV_N16 (1.0f / 8.0f)
+
+// The collision: the reference's MRT with Guo forcing,
+//   f' = f + M^-1 S M n + fg - 0.5 M^-1 S M fg,  n = f_eq - f
+// (GPU_program.cl:396-623), evaluated as one forward and one inverse
+// transform of d = n - fg/2 (linearity):  f' = f + fg + M^T D^-1 S M d.
+// The density row carries no relaxation term (S_rho = 0).  The momentum rows
+// are kept although M_j d = (rho u - j) - g/2 vanishes in exact arithmetic:
+// relaxed with rate 1 they move j onto the first moment of the rounded f_eq
+// every step, as the reference does, instead of letting that rounding
+// difference accumulate as a momentum drift.  COLL 0: the reference's rate
+// vector with 1/tau at rows 8,9,10,14,15 (GPU_program.cl:453, 567-568);
+// COLL 1: BGK.
+template <int COLL, bool VAR>
+__device__ __forceinline__ void collide(float (&f)[19], float rho, float ux, float uy, float uz, float gx, float gy,
+                                        float gz, float& tau, const FluidParams& p, bool& clamped) {
+  // Equilibrium minus f, pairwise (GPU_program.cl:978-1007), and the Guo term
+  // (GPU_program.cl:1010-1038): for a pair +-c the even parts are shared.
+  const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+  const float uDg = ux * gx + uy * gy + uz * gz;
+  const float r0 = rho / 3.0f, r1 = rho / 18.0f, r2 = rho / 36.0f;
+  float d[19], base[19];
+  {
+    float feq0 = r0 * (1.0f - usq15);
+    float fg0 = -uDg;
+    d[0] = (feq0 - f[0]) - 0.5f * fg0;
+    base[0] = f[0] + fg0;
+  }
+#define PAIR(qp, qm, cu, cg, rw, gd)                                   \
+  {                                                                   \
+    const float cu_ = (cu), cg_ = (cg);                               \
+    const float ev = (rw) * (1.0f + 4.5f * cu_ * cu_ - usq15);        \
+    const float od = (rw) * (3.0f * cu_);                             \
+    const float gev = (-uDg + 3.0f * cu_ * cg_) * (1.0f / (gd));      \
+    const float god = cg_ * (1.0f / (gd));                            \
+    const float fgp = gev + god, fgm = gev - god;                     \
+    d[qp] = ((ev + od) - f[qp]) - 0.5f * fgp;                         \
+    d[qm] = ((ev - od) - f[qm]) - 0.5f * fgm;                         \
+    base[qp] = f[qp] + fgp;                                           \
+    base[qm] = f[qm] + fgm;                                           \
+  }
+  PAIR(1, 2, ux, gx, r1, 6.0f)
+  PAIR(3, 4, uy, gy, r1, 6.0f)
+  PAIR(5, 6, uz, gz, r1, 6.0f)
+  PAIR(7, 12, ux + uy, gx + gy, r2, 12.0f)
+  PAIR(8, 11, ux - uy, gx - gy, r2, 12.0f)
+  PAIR(9, 14, ux + uz, gx + gz, r2, 12.0f)
+  PAIR(10, 13, ux - uz, gx - gz, r2, 12.0f)
+  PAIR(15, 18, uy + uz, gy + gz, r2, 12.0f)
+  PAIR(16, 17, uy - uz, gy - gz, r2, 12.0f)
+#undef PAIR
+
+  // Forward transform of d (non-conserved rows only), butterfly form.
+  const float Ax = d[1] + d[2], Bx = d[1] - d[2];
+  const float Ay = d[3] + d[4], By = d[3] - d[4];
+  const float Az = d[5] + d[6], Bz = d[5] - d[6];
+  float Sxy, Xxy, Yxy, Pxy, Sxz, Xxz, Zxz, Pxz, Syz, Yyz, Zyz, Pyz;
+  {
+    float a = d[7] + d[8], b = d[11] + d[12], c = d[7] - d[8], e = d[11] - d[12];
+    Sxy = a + b; Xxy = a - b; Yxy = c + e; Pxy = c - e;
+  }
+  {
+    float a = d[9] + d[10], b = d[13] + d[14], c = d[9] - d[10], e = d[13] - d[14];
+    Sxz = a + b; Xxz = a - b; Zxz = c + e; Pxz = c - e;
+  }
+  {
+    float a = d[15] + d[16], b = d[17] + d[18], c = d[15] - d[16], e = d[17] - d[18];
+    Syz = a + b; Yyz = a - b; Zyz = c + e; Pyz = c - e;
+  }
+  const float A = Ax + Ay + Az, S = Sxy + Sxz + Syz;
+  const float m1 = -30.0f * d[0] - 11.0f * A + 8.0f * S;
+  const float m2 = 12.0f * d[0] - 4.0f * A + S;
+  const float m3 = Bx + Xxy + Xxz;
+  const float m5 = By + Yxy + Yyz;
+  const float m7 = Bz + Zxz + Zyz;
+  const float m4 = -4.0f * Bx + Xxy + Xxz;
+  const float m6 = -4.0f * By + Yxy + Yyz;
+  const float m8 = -4.0f * Bz + Zxz + Zyz;
+  const float T9 = Sxy + Sxz - 2.0f * Syz;
+  const float m9 = 2.0f * Ax - Ay - Az + T9;
+  const float m10 = -4.0f * Ax + 2.0f * Ay + 2.0f * Az + T9;
+  const float T11 = Sxy - Sxz;
+  const float m11 = Ay - Az + T11;
+  const float m12 = -2.0f * Ay + 2.0f * Az + T11;
+  const float m13 = Pxy, m14 = Pyz, m15 = Pxz;
+  const float m16 = Xxy - Xxz, m17 = Yyz - Yxy, m18 = Zxz - Zyz;
+
+  // Rates.
+  float s1, s2, s4, s6, s11, s12, s13, s16;
+  if (COLL == 0) {
+    s1 = 1.19f; s2 = 1.40f; s4 = 1.20f; s6 = 1.20f; s11 = 1.20f; s12 = 1.40f; s13 = 1.40f; s16 = 1.98f;
+  }
+
+  if (VAR) {
+    // Strain rate from the relaxed non-equilibrium moments with tau(t-1)
+    // (GPU_program.cl:459-562): the second moments of M^-1 S_old M d, which
+    // only rows e, 3pxx, pww and the off-diagonal p carry.
+    const float it = 1.0f / tau;
+    float a1, a9, a11, a13, a14, a15;
+    if (COLL == 0) {
+      a1 = s1 * m1 * INV_N1; a9 = it * m9 * INV_N9; a11 = s11 * m11 * INV_N11;
+      a13 = s13 * m13 * INV_N13; a14 = it * m14 * INV_N13; a15 = it * m15 * INV_N13;
+    } else {
+      a1 = it * m1 * INV_N1; a9 = it * m9 * INV_N9; a11 = it * m11 * INV_N11;
+      a13 = it * m13 * INV_N13; a14 = it * m14 * INV_N13; a15 = it * m15 * INV_N13;
+    }
+    const float sxx = 42.0f * a1 + 12.0f * a9;
+    const float syy = 42.0f * a1 - 6.0f * a9 + 6.0f * a11;
+    const float szz = 42.0f * a1 - 6.0f * a9 - 6.0f * a11;
+    const float sxy = 4.0f * a13, syz = 4.0f * a14, sxz = 4.0f * a15;
+    const float ss = sxx * sxx + 2.0f * (sxy * sxy + sxz * sxz + syz * syz) + syy * syy + szz * szz;
+    const float srt = sqrtf(ss) * 2.1213203f / rho;
+    tau = compute_tau(p, srt, clamped);
+  }
+
+  const float it = 1.0f / tau;
+  float a1, a2, a3, a4, a5, a6, a7, a8, a9, a10, a11, a12, a13, a14, a15, a16, a17, a18;
+  if (COLL == 0) {
+    a3 = 0.1f * m3; a5 = 0.1f * m5; a7 = 0.1f * m7;
+    a1 = s1 * INV_N1 * m1; a2 = s2 * INV_N2 * m2; a4 = s4 * INV_N4 * m4; a6 = s6 * INV_N4 * m6;
+    a8 = it * INV_N4 * m8; a9 = it * INV_N9 * m9; a10 = it * INV_N10 * m10; a11 = s11 * INV_N11 * m11;
+    a12 = s12 * INV_N12 * m12; a13 = s13 * INV_N13 * m13; a14 = it * INV_N13 * m14; a15 = it * INV_N13 * m15;
+    a16 = s16 * INV_N16 * m16; a17 = s16 * INV_N16 * m17; a18 = s16 * INV_N16 * m18;
+  } else {
+    a3 = it * 0.1f * m3; a5 = it * 0.1f * m5; a7 = it * 0.1f * m7;
+    a1 = it * INV_N1 * m1; a2 = it * INV_N2 * m2; a4 = it * INV_N4 * m4; a6 = it * INV_N4 * m6;
+    a8 = it * INV_N4 * m8; a9 = it * INV_N9 * m9; a10 = it * INV_N10 * m10; a11 = it * INV_N11 * m11;
+    a12 = it * INV_N12 * m12; a13 = it * INV_N13 * m13; a14 = it * INV_N13 * m14; a15 = it * INV_N13 * m15;
+    a16 = it * INV_N16 * m16; a17 = it * INV_N16 * m17; a18 = it * INV_N16 * m18;
+  }
+
+  // Inverse transform M^T a, butterfly form.
+  f[0] = base[0] + (-30.0f * a1 + 12.0f * a2);
+  const float bax = -11.0f * a1 - 4.0f * a2;
+  const float Cx = bax + 2.0f * a9 - 4.0f * a10;
+  const float Cy = bax - a9 + 2.0f * a10 + a11 - 2.0f * a12;
+  const float Cz = bax - a9 + 2.0f * a10 - a11 + 2.0f * a12;
+  const float Ox = a3 - 4.0f * a4, Oy = a5 - 4.0f * a6, Oz = a7 - 4.0f * a8;
+  f[1] = base[1] + (Cx + Ox);
+  f[2] = base[2] + (Cx - Ox);
+  f[3] = base[3] + (Cy + Oy);
+  f[4] = base[4] + (Cy - Oy);
+  f[5] = base[5] + (Cz + Oz);
+  f[6] = base[6] + (Cz - Oz);
+  const float bd = 8.0f * a1 + a2;
+  {  // xy: 7 (+,+) 8 (+,-) 11 (-,+) 12 (-,-)
+    const float E = bd + a9 + a10 + a11 + a12, X = a3 + a4 + a16, Y = a5 + a6 - a17, P = a13;
+    const float u1 = E + P, u2 = E - P, v1 = X + Y, v2 = X - Y;
+    f[7] = base[7] + (u1 + v1); f[12] = base[12] + (u1 - v1);
+    f[8] = base[8] + (u2 + v2); f[11] = base[11] + (u2 - v2);
+  }
+  {  // xz: 9 (+,+) 10 (+,-) 13 (-,+) 14 (-,-)
+    const float E = bd + a9 + a10 - a11 - a12, X = a3 + a4 - a16, Z = a7 + a8 + a18, P = a15;
+    const float u1 = E + P, u2 = E - P, v1 = X + Z, v2 = X - Z;
+    f[9] = base[9] + (u1 + v1); f[14] = base[14] + (u1 - v1);
+    f[10] = base[10] + (u2 + v2); f[13] = base[13] + (u2 - v2);
+  }
+  {  // yz: 15 (+,+) 16 (+,-) 17 (-,+) 18 (-,-)
+    const float E = bd - 2.0f * a9 - 2.0f * a10, Y = a5 + a6 + a17, Z = a7 + a8 - a18, P = a14;
+    const float u1 = E + P, u2 = E - P, v1 = Y + Z, v2 = Y - Z;
+    f[15] = base[15] + (u1 + v1); f[18] = base[18] + (u1 - v1);
+    f[16] = base[16] + (u2 + v2); f[17] = base[17] + (u2 - v2);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Spread force of one tile: accumulate -w*F of every listed marker on the
+// tile plus a one-node halo (the reference's gpf slot sum, GPU_program.cl:
+// 210-227 and 258-289) in 2^-40 fixed point, then convert to float.
+struct SpreadSmem {
+  int hi[3][HALO_N];        // sum of the high parts (v >> 16)
+  unsigned lo[3][HALO_N];   // sum of the low 16 bits
+  float g[3][HALO_N];       // the spread force of the halo nodes
+};
+
+__device__ __forceinline__ void marker_weights(float wx, float wy, float wz, float (&w)[8]) {
+  // GPU_program.cl:170-178.
+  w[0] = wx * wy * wz;
+  w[1] = (1.0f - wx) * wy * wz;
+  w[2] = wx * (1.0f - wy) * wz;
+  w[3] = wx * wy * (1.0f - wz);
+  w[4] = (1.0f - wx) * (1.0f - wy) * wz;
+  w[5] = (1.0f - wx) * wy * (1.0f - wz);
+  w[6] = wx * (1.0f - wy) * (1.0f - wz);
+  w[7] = (1.0f - wx) * (1.0f - wy) * (1.0f - wz);
+}
+
+__device__ __forceinline__ void decode_marker(const float4& a, const float4& b, int& x0, int& y0, int& z0) {
+  const unsigned xy = __float_as_uint(a.w);
+  x0 = (int)(xy & 0xffffu);
+  y0 = (int)(xy >> 16);
+  z0 = (int)__float_as_uint(b.w);
+}
+
+// Fixed-point unit of the step whose markers are listed, as a power of two
+// 2^k with max|force| * 2^k < 2^FIX_BITS.
+__device__ __forceinline__ int fixed_exponent(unsigned fmax_bits) {
+  const float fm = __uint_as_float(fmax_bits);
+  if (!(fm > 0.0f)) return 0;
+  int e;
+  frexpf(fm, &e);  // fm < 2^e
+  return FIX_BITS - e;
+}
+
+// Accumulates the tile's listed markers into s (X0,Y0,Z0 = tile origin) and
+// leaves the halo's spread force in s.g.  Every contribution -w*F (the
+// reference's "gpf -= weights[n]*vuForce", GPU_program.cl:222-224) is scaled
+// by 2^k (exact), rounded to an integer and summed exactly in two 32-bit
+// parts; the sum is converted back once.
+__device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& tl, long long T, int n, int X0,
+                                int Y0, int Z0, int tid, int nthreads, int k, unsigned* err) {
+  for (int h = tid; h < 3 * HALO_N; h += nthreads) {
+    (&s.hi[0][0])[h] = 0;
+    (&s.lo[0][0])[h] = 0u;
+  }
+  __syncthreads();
+  const float scale = ldexpf(1.0f, k);
+  for (int j = tid; j < n; j += nthreads) {
+    const int m = tl.list[T * tl.cap + j];
+    const float4 a = tl.mrec[2 * (long long)m], b = tl.mrec[2 * (long long)m + 1];
+    int x0, y0, z0;
+    decode_marker(a, b, x0, y0, z0);
+    const int xs = (x0 == g.Nx - 2) ? -(g.Nx - 3) : 1;
+    const int ys = (y0 == g.Ny - 2) ? -(g.Ny - 3) : 1;
+    const int zs = (z0 == g.Nz - 2) ? -(g.Nz - 3) : 1;
+    float w[8];
+    marker_weights(a.x, a.y, a.z, w);
+    const int sh[8][3] = {{0, 0, 0}, {xs, 0, 0}, {0, ys, 0}, {0, 0, zs}, {xs, ys, 0}, {xs, 0, zs}, {0, ys, zs},
+                          {xs, ys, zs}};
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int hx = x0 + sh[q][0] - (X0 - 1), hy = y0 + sh[q][1] - (Y0 - 1), hz = z0 + sh[q][2] - (Z0 - 1);
+      if (hx < 0 || hx >= HALO_X || hy < 0 || hy >= HALO_Y || hz < 0 || hz >= HALO_Z) continue;
+      const int h = hx + HALO_X * (hy + HALO_Y * hz);
+      const float c[3] = {w[q] * b.x, w[q] * b.y, w[q] * b.z};
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const float sv = -c[d] * scale;  // exact: power-of-two scaling
+        if (!(fabsf(sv) < 549755813888.0f)) {  // 2^39
+          atomicOr(err, ERR_FIXED_RANGE);
+          continue;
+        }
+        const long long v = __float2ll_rn(sv);
+        atomicAdd(&s.hi[d][h], (int)(v >> 16));
+        atomicAdd(&s.lo[d][h], (unsigned)(v & 0xffff));
+      }
+    }
+  }
+  __syncthreads();
+  const float inv = ldexpf(1.0f, -k);
+  for (int h = tid; h < 3 * HALO_N; h += nthreads) {
+    const long long v = (long long)(&s.hi[0][0])[h] * 65536LL + (long long)(&s.lo[0][0])[h];
+    (&s.g[0][0])[h] = __ll2float_rn(v) * inv;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+template <bool FIRST, bool VAR, int COLL>
+__global__ void __launch_bounds__(FLUID_THREADS, 4) fluid_step_kernel(const FluidArgs a) {
+  __shared__ SpreadSmem sm;
+  __shared__ int s_cnt;
+  const Geom& g = a.g;
+  const int tid = threadIdx.x + TILE_X * (threadIdx.y + TILE_Y * threadIdx.z);
+  const int nthreads = FLUID_THREADS;
+  const int X0 = blockIdx.x * TILE_X, Y0 = blockIdx.y * TILE_Y, Z0 = blockIdx.z * TILE_Z;
+  const long long T = blockIdx.x + (long long)g.ntx * (blockIdx.y + (long long)g.nty * blockIdx.z);
+
+  int cnt = 0;
+  if (a.has_ibm) {
+    if (tid == 0) s_cnt = a.tiles.count[T];
+    __syncthreads();
+    cnt = s_cnt;
+    // The markers listed now are those of step t-1; the particle pass of
+    // step t records its force maximum in the other slot, cleared here.
+    const unsigned fbits = a.tiles.fmax[(a.t + 1) & 1];
+    if (T == 0 && tid == 0) a.tiles.fmax[a.t & 1] = 0u;
+    if (cnt > 0) {
+      __syncthreads();
+      if (tid == 0) a.tiles.count[T] = 0;  // consumed; the particle pass of this step refills it
+      accumulate_tile(sm, g, a.tiles, T, min(cnt, a.tiles.cap), X0, Y0, Z0, tid, nthreads, fixed_exponent(fbits),
+                      a.err);
+    }
+  }
+
+  const int x = X0 + threadIdx.x;
+  const int y = Y0 + threadIdx.y;
+  const long long NC = g.NC;
+  const float sten[3] = {0.25f, 0.5f, 0.25f};
+  int nclamp = 0;
+#pragma unroll 1
+  for (int zz = 0; zz < TILE_Z / 2; zz++) {
+    const int z = Z0 + threadIdx.z + 2 * zz;
+    if (x < 1 || x > g.Nx - 2 || y < 1 || y > g.Ny - 2 || z < 1 || z > g.Nz - 2) continue;
+    const long long i = x + (long long)g.Nx * (y + (long long)g.Ny * z);
+    float f[19];
+    if (FIRST) {
+#pragma unroll
+      for (int q = 0; q < 19; q++) f[q] = __ldg(a.fin + q * NC + i);
+    } else {
+      int dxm, dxp, dym, dyp, dzm, dzp;
+      neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
+      gather(f, a.fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp);
+      boundaries(f, g, a.p, x, y, z);
+    }
+    float gx = a.p.g[0], gy = a.p.g[1], gz = a.p.g[2];
+    if (cnt > 0) {
+      const int hx = x - X0 + 1, hy = y - Y0 + 1, hz = z - Z0 + 1;
+#pragma unroll
+      for (int sx = -1; sx <= 1; sx++)
+#pragma unroll
+        for (int sy = -1; sy <= 1; sy++)
+#pragma unroll
+          for (int sz = -1; sz <= 1; sz++) {
+            const float ws = sten[sx + 1] * sten[sy + 1] * sten[sz + 1];
+            const int h = (hx + sx) + HALO_X * ((hy + sy) + HALO_Y * (hz + sz));
+            gx += ws * sm.g[0][h];
+            gy += ws * sm.g[1][h];
+            gz += ws * sm.g[2][h];
+          }
+    }
+    float rho = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 19; q++) rho += f[q];
+    const float jx = f[1] - f[2] + f[7] + f[8] + f[9] + f[10] - f[11] - f[12] - f[13] - f[14];
+    const float jy = f[3] - f[4] + f[7] - f[8] + f[11] - f[12] + f[15] + f[16] - f[17] - f[18];
+    const float jz = f[5] - f[6] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16] + f[17] - f[18];
+    const float ux = (jx + 0.5f * gx) / rho, uy = (jy + 0.5f * gy) / rho, uz = (jz + 0.5f * gz) / rho;
+    a.u[i] = ux;
+    a.u[i + NC] = uy;
+    a.u[i + 2 * NC] = uz;
+    if (!(fabsf(ux) + fabsf(uy) + fabsf(uz) < 1e30f) || !(rho > 0.0f)) atomicOr(a.err, ERR_NONFINITE);
+    float tau = VAR ? a.tau[i] : a.p.tauN;
+    bool clamped = false;
+    collide<COLL, VAR>(f, rho, ux, uy, uz, gx, gy, gz, tau, a.p, clamped);
+    if (VAR) {
+      a.tau[i] = tau;
+      nclamp += clamped ? 1 : 0;
+    }
+#pragma unroll
+    for (int q = 0; q < 19; q++) a.fout[q * NC + i] = f[q];
+  }
+  if (VAR && nclamp) atomicAdd(a.clamps, (unsigned long long)nclamp);
+}
+
+// Post-streaming, post-boundary populations of the last step (what the
+// reference's f_s holds after its boundary kernels), for read-back.
+__global__ void materialize_f_kernel(const FluidArgs a, float* __restrict__ out) {
+  const Geom& g = a.g;
+  const long long NC = g.NC;
+  const long long n = (long long)(g.Nx - 2) * (g.Ny - 2) * (g.Nz - 2);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int x = 1 + (int)(k % (g.Nx - 2));
+    const int y = 1 + (int)((k / (g.Nx - 2)) % (g.Ny - 2));
+    const int z = 1 + (int)(k / ((long long)(g.Nx - 2) * (g.Ny - 2)));
+    const long long i = x + (long long)g.Nx * (y + (long long)g.Ny * z);
+    int dxm, dxp, dym, dyp, dzm, dzp;
+    neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
+    float f[19];
+    gather(f, a.fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp);
+    boundaries(f, g, a.p, x, y, z);
+#pragma unroll
+    for (int q = 0; q < 19; q++) out[q * NC + i] = f[q];
+  }
+}
+
+// Dense spread-force field (the reference's gpf slot 0) from the tile lists,
+// for parity read-back.  One block per tile; does not consume the lists.
+__global__ void __launch_bounds__(256) spread_field_kernel(const Geom g, const TileLists tl, int last_step,
+                                                           float* __restrict__ out, unsigned* err) {
+  __shared__ SpreadSmem sm;
+  const int tid = threadIdx.x;
+  const long long T = blockIdx.x + (long long)g.ntx * (blockIdx.y + (long long)g.nty * blockIdx.z);
+  const int X0 = blockIdx.x * TILE_X, Y0 = blockIdx.y * TILE_Y, Z0 = blockIdx.z * TILE_Z;
+  const int cnt = tl.count[T];
+  if (cnt <= 0) return;
+  accumulate_tile(sm, g, tl, T, min(cnt, tl.cap), X0, Y0, Z0, tid, blockDim.x,
+                  fixed_exponent(tl.fmax[last_step & 1]), err);
+  for (int k = tid; k < TILE_X * TILE_Y * TILE_Z; k += blockDim.x) {
+    const int x = X0 + k % TILE_X, y = Y0 + (k / TILE_X) % TILE_Y, z = Z0 + k / (TILE_X * TILE_Y);
+    if (x < 1 || x > g.Nx - 2 || y < 1 || y > g.Ny - 2 || z < 1 || z > g.Nz - 2) continue;
+    const long long i = x + (long long)g.Nx * (y + (long long)g.Ny * z);
+    const int h = (x - X0 + 1) + HALO_X * ((y - Y0 + 1) + HALO_Y * (z - Z0 + 1));
+    out[i] = sm.g[0][h];
+    out[i + g.NC] = sm.g[1][h];
+    out[i + 2 * g.NC] = sm.g[2][h];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Particles.  Float arithmetic of the rigid-body update and the marker
+// placement uses explicitly rounded operations (no contraction) so that the
+// same update evaluated in different blocks is bit-identical and follows the
+// reference's IEEE evaluation order.
+__device__ __forceinline__ float4 f4add(float4 a, float4 b) {
+  return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w));
+}
+__device__ __forceinline__ float4 f4sub(float4 a, float4 b) {
+  return make_float4(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z), __fsub_rn(a.w, b.w));
+}
+__device__ __forceinline__ float4 f4mul(float4 a, float s) {
+  return make_float4(__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s), __fmul_rn(a.w, s));
+}
+__device__ __forceinline__ float4 f4div(float4 a, float s) {
+  return make_float4(__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s), __fdiv_rn(a.w, s));
+}
+__device__ __forceinline__ float4 f4cross(float4 a, float4 b) {
+  return make_float4(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+                     __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+                     __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)), 0.0f);
+}
+
+struct Kin {
+  float4 x, v, q, w;
+};
+
+// particle_dynamics for one sphere (CPU_program.cl:209-276).
+__device__ Kin rigid_update(const ParticleArgs& a, int p) {
+  const ParticleParams& P = a.p;
+  const int np = P.np, nfa = P.nfa;
+  Kin k;
+  k.x = a.kin_old[p];
+  k.v = a.kin_old[p + np];
+  k.q = a.kin_old[p + 2 * np];
+  k.w = a.kin_old[p + 3 * np];
+  if (P.fixed) return k;
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f), aacc = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int fa = 0; fa < nfa; fa++) {
+    acc = f4add(acc, a.pff_old[p * nfa + fa]);
+    aacc = f4add(aacc, a.pff_old[(p + np) * nfa + fa]);
+  }
+  acc = f4add(acc, a.pf_old[p]);
+  aacc = f4add(aacc, a.pf_old[p + np]);
+  acc = f4div(acc, P.mass);
+  aacc = f4div(aacc, P.inertia);
+  acc.x = __fadd_rn(acc.x, P.g[0]);
+  acc.y = __fadd_rn(acc.y, P.g[1]);
+  acc.z = __fadd_rn(acc.z, P.g[2]);
+  const float4 W = make_float4(P.S[0], P.S[1], P.S[2], 1.0f);
+  const float4 rt = f4add(f4add(k.x, k.v), f4mul(acc, 0.5f));
+  const float4 rw = f4add(rt, W);
+  Kin o;
+  o.x = make_float4(fmodf(rw.x, W.x), fmodf(rw.y, W.y), fmodf(rw.z, W.z), fmodf(rw.w, W.w));
+  o.v = f4add(k.v, acc);
+  const float dqw = -__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(k.w.x, k.q.x), __fmul_rn(k.w.y, k.q.y)),
+                                         __fmul_rn(k.w.z, k.q.z)),
+                               __fmul_rn(k.w.w, k.q.w));
+  const float4 dq = f4add(f4mul(k.w, k.q.w), f4cross(k.w, k.q));
+  o.q = f4mul(dq, 0.5f);
+  o.q.w = __fadd_rn(o.q.w, __fmul_rn(0.5f, dqw));
+  o.w = f4add(k.w, aacc);
+  return o;
+}
+
+// Tile indices along one axis whose halo contains node coordinate c.
+__device__ __forceinline__ void tile_range(int c, int T, int nt, int& lo, int& hi) {
+  lo = (c + T - 1) / T - 1;
+  if (lo < 0) lo = 0;
+  hi = (c + 1) / T;
+  if (hi > nt - 1) hi = nt - 1;
+}
+
+// Distinct tile indices covering two node coordinates (at most 4).
+__device__ __forceinline__ int tile_set(int c0, int c1, int T, int nt, int (&out)[4]) {
+  int l0, h0, l1, h1, n = 0;
+  tile_range(c0, T, nt, l0, h0);
+  tile_range(c1, T, nt, l1, h1);
+  for (int t = l0; t <= h0 && n < 4; t++) out[n++] = t;
+  for (int t = l1; t <= h1 && n < 4; t++) {
+    bool dup = false;
+    for (int j = 0; j < n; j++) dup |= out[j] == t;
+    if (!dup) out[n++] = t;
+  }
+  return n;
+}
+
+// Pair force of the reference's contact loop (CPU_program.cl:118-169) for
+// the pair (A, B), A the higher sphere index: unit vector e (A to B, nearest
+// periodic image in x, y and z) and the total magnitude along e (harmonic
+// overlap + Newtonian squeeze film; the two exclude each other).
+__device__ bool pair_force(const ParticleParams& P, const Kin& A, const Kin& B, float4& e, float& fmag) {
+  const float rp = P.diam / 2.0f;
+  float4 rij = f4sub(B.x, A.x);
+  float* r = &rij.x;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const int sg = (r[d] < 0.0f) ? -1 : (r[d] > 0.0f);
+    r[d] = (fabsf(r[d]) < P.S[d] / 2.0f) ? r[d] : __fsub_rn(r[d], __fmul_rn((float)sg, P.S[d]));
+  }
+  const float rSep = sqrtf(__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(rij.x, rij.x), __fmul_rn(rij.y, rij.y)),
+                                               __fmul_rn(rij.z, rij.z)),
+                                     __fmul_rn(rij.w, rij.w)));
+  const float4 vij = f4sub(B.v, A.v);
+  const float minSep = __fsub_rn(rSep, 2.0f * rp);
+  e = f4div(rij, rSep);
+  const float vRel = -__fadd_rn(__fadd_rn(__fmul_rn(e.x, vij.x), __fmul_rn(e.y, vij.y)), __fmul_rn(e.z, vij.z));
+  fmag = 0.0f;
+  bool any = false;
+  const float overlap = -minSep;
+  if (overlap > 0 && P.forceModel == 1) {
+    fmag = __fmul_rn(P.kcol, overlap);
+    any = true;
+  }
+  if (minSep > 0 && (double)minSep < 0.1 * (double)rp) {
+    float sq = 0.0f;
+    if (P.viscModel == 1) {  // compute_squeeze_force, CPU_program.cl:319-343
+      const float rStar = rp / 2.0f;
+      const float ms = minSep < 0.1f ? 0.1f : minSep;
+      const double eta0 = (double)((P.tauN - 0.5f) / 3.0f);
+      sq = (float)(6.0 * 3.14159265358979323846 * eta0 * rStar * rStar * vRel / ms);
+    }
+    fmag = any ? __fadd_rn(fmag, sq) : sq;
+    any = true;
+  }
+  return any;
+}
+
+// One block per reference work-group of markers (blocks [0, np*nfa)), then
+// blocks of warps for the particle-particle forces, one warp per sphere.
+__global__ void particle_step_kernel(const ParticleArgs a) {
+  extern __shared__ float4 red[];  // [2*blockDim.x]: forces, then torques
+  const ParticleParams& P = a.p;
+  const Geom& g = a.g;
+  const int np = P.np, nfa = P.nfa, L = P.L;
+  const int ngroups = np * nfa;
+  const int l = threadIdx.x;
+  const int lane = l & 31;
+  if ((int)blockIdx.x < ngroups) {
+    const int grp = blockIdx.x;
+    const int p = grp / nfa;
+    const Kin k = rigid_update(a, p);
+    if (grp % nfa == 0 && l == 0) {
+      a.kin_new[p] = k.x;
+      a.kin_new[p + np] = k.v;
+      a.kin_new[p + 2 * np] = k.q;
+      a.kin_new[p + 3 * np] = k.w;
+    }
+    float4 force = make_float4(0.f, 0.f, 0.f, 0.f), torque = force;
+    int tx[4], ty[4], tz[4], nx = 0, ny = 0, nz = 0;
+    long long gid = (long long)grp * L + l;
+    if (l < L) {
+      const int pt = (int)(gid % P.P);
+      const float4 r0 = a.sphere[pt];
+      const float4 W = make_float4(P.S[0], P.S[1], P.S[2], 1.0f);
+      const float4 rw = f4add(f4add(k.x, r0), W);
+      const float4 rpp = make_float4(fmodf(rw.x, W.x), fmodf(rw.y, W.y), fmodf(rw.z, W.z), fmodf(rw.w, W.w));
+      const float fx = floorf(rpp.x), fy = floorf(rpp.y), fz = floorf(rpp.z);
+      const int x0 = (int)fx + P.buffer[0], y0 = (int)fy + P.buffer[1], z0 = (int)fz + P.buffer[2];
+      const bool ok = fx == fx && fy == fy && fz == fz && x0 >= 1 && x0 <= g.Nx - 2 && y0 >= 1 &&
+                      y0 <= g.Ny - 2 && z0 >= 1 && z0 <= g.Nz - 2;
+      if (!ok) {
+        atomicOr(a.err, ERR_NONFINITE);
+      } else {
+        const int xs = (x0 == g.Nx - 2) ? -(g.Nx - 3) : 1;
+        const int ys = (y0 == g.Ny - 2) ? -(g.Ny - 3) : 1;
+        const int zs = (z0 == g.Nz - 2) ? -(g.Nz - 3) : 1;
+        const float wx = __fsub_rn(1.0f, __fsub_rn(rpp.x, fx));
+        const float wy = __fsub_rn(1.0f, __fsub_rn(rpp.y, fy));
+        const float wz = __fsub_rn(1.0f, __fsub_rn(rpp.z, fz));
+        float w[8];
+        marker_weights(wx, wy, wz, w);
+        const int sh[8][3] = {{0, 0, 0}, {xs, 0, 0}, {0, ys, 0}, {0, 0, zs}, {xs, ys, 0}, {xs, 0, zs},
+                              {0, ys, zs}, {xs, ys, zs}};
+        float ux = 0.f, uy = 0.f, uz = 0.f;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const long long i =
+              (x0 + sh[j][0]) + (long long)g.Nx * ((y0 + sh[j][1]) + (long long)g.Ny * (z0 + sh[j][2]));
+          // GPU_program.cl:193-195, without contraction.
+          ux = __fadd_rn(ux, __fmul_rn(w[j], a.u[i]));
+          uy = __fadd_rn(uy, __fmul_rn(w[j], a.u[i + g.NC]));
+          uz = __fadd_rn(uz, __fmul_rn(w[j], a.u[i + 2 * g.NC]));
+        }
+        const float4 upp = make_float4(ux, uy, uz, 0.0f);
+        const float4 vpp = f4add(k.v, f4cross(k.w, r0));
+        force = f4mul(f4sub(upp, vpp), P.pointArea);
+        torque = f4cross(r0, force);
+        a.mrec[2 * gid] = make_float4(wx, wy, wz, __uint_as_float((unsigned)x0 | ((unsigned)y0 << 16)));
+        a.mrec[2 * gid + 1] = make_float4(force.x, force.y, force.z, __uint_as_float((unsigned)z0));
+        nx = tile_set(x0, x0 + xs, TILE_X, g.ntx, tx);
+        ny = tile_set(y0, y0 + ys, TILE_Y, g.nty, ty);
+        nz = tile_set(z0, z0 + zs, TILE_Z, g.ntz, tz);
+      }
+    }
+    // List the marker in every fluid tile whose halo holds one of its
+    // stencil nodes; lanes inserting into the same tile share one atomic.
+    {
+      const int n = nx * ny * nz;
+      int nmax = n;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+      for (int j = 0; j < nmax; j++) {
+        const bool act = j < n;
+        const unsigned amask = __ballot_sync(0xffffffffu, act);
+        if (act) {
+          const int ia = j % nx, ib = (j / nx) % ny, ic = j / (nx * ny);
+          const int T = tx[ia] + g.ntx * (ty[ib] + g.nty * tz[ic]);
+          const unsigned peers = __match_any_sync(amask, T);
+          const int leader = __ffs(peers) - 1;
+          int base = 0;
+          if (lane == leader) base = atomicAdd(&a.tiles.count[T], __popc(peers));
+          base = __shfl_sync(peers, base, leader);
+          const int slot = base + __popc(peers & ((1u << lane) - 1u));
+          if (slot < a.tiles.cap) a.tiles.list[(long long)T * a.tiles.cap + slot] = (int)gid;
+          else atomicOr(a.err, ERR_TILE_OVERFLOW);
+        }
+      }
+    }
+    // Largest force component of the step (fixed-point unit of the spread):
+    // warp maximum, then one atomic per warp.
+    {
+      float fm = fmaxf(fabsf(force.x), fmaxf(fabsf(force.y), fabsf(force.z)));
+      if (!(fm == fm)) fm = 3.0e38f;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) fm = fmaxf(fm, __shfl_xor_sync(0xffffffffu, fm, o));
+      if (lane == 0 && fm > 0.0f) atomicMax(&a.tiles.fmax[a.t & 1], __float_as_uint(fm));
+    }
+    // Work-group reduction in the reference's tree order
+    // (GPU_program.cl:232-255).
+    const int B = blockDim.x;
+    red[l] = force;
+    red[l + B] = torque;
+    __syncthreads();
+    for (int s = L / 2; s > 0; s >>= 1) {
+      if (l < s) {
+        red[l] = f4add(red[l], red[l + s]);
+        red[l + B] = f4add(red[l + B], red[l + s + B]);
+      }
+      __syncthreads();
+    }
+    if (l == 0) {
+      a.pff_new[grp] = red[0];
+      a.pff_new[grp + ngroups] = red[B];
+    }
+    return;
+  }
+
+  // Particle-particle forces (CPU_program.cl:76-184), one warp per sphere pi:
+  // every pair occurrence the reference's zone loops produce for pi, as the
+  // higher index (neighbour zones of pi's zone, members pj < pi; lane t takes
+  // neighbour entry t) and as the lower one (zones whose neighbour list names
+  // pi's zone, members pk > pi; lanes over the reverse table), then a fixed
+  // shuffle reduction: deterministic.
+  const int pi = (blockIdx.x - ngroups) * (blockDim.x / 32) + (l >> 5);
+  if (pi >= np) return;  // whole warps
+  const int nzones = P.numZones[0] * P.numZones[1] * P.numZones[2];
+  const Kin ki = rigid_update(a, pi);
+  float4 F = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int pz = a.parsZone[pi];
+  if (P.exact) {
+    // The reference's accumulation order (serial work-items, spheres in
+    // increasing index): pi's own pairs in zone/member order, its wall
+    // terms, then the pairs of every higher sphere that names pi.
+    if (lane != 0) return;
+    if (pz >= 0 && pz < nzones) {
+      for (int t = 1; t <= a.znd[28 * pz]; t++) {
+        const int zid = a.znd[28 * pz + t];
+        if (zid < 0 || zid >= nzones) continue;
+        for (int j = 0; j < a.numParInZone[zid]; j++) {
+          const int pj = a.zoneMembers[zid * np + j];
+          if (!(pi > pj)) continue;
+          const Kin kj = rigid_update(a, pj);
+          float4 e;
+          float fm;
+          if (pair_force(P, ki, kj, e, fm)) F = f4sub(F, f4mul(e, fm));
+        }
+      }
+    }
+    const float lo = __fsub_rn(P.zbuf, ki.x.z);
+    if (lo > 0) F.z = __fadd_rn(F.z, __fmul_rn(P.kcol, lo));
+    const float up = __fsub_rn(ki.x.z, __fsub_rn((float)P.Sint[2], P.zbuf));
+    if (up > 0) F.z = __fsub_rn(F.z, __fmul_rn(P.kcol, up));
+    if (pz >= 0 && pz < nzones) {
+      for (int pk = pi + 1; pk < np; pk++) {
+        const int Y = a.parsZone[pk];
+        if (Y < 0 || Y >= nzones) continue;
+        bool have = false;
+        Kin kk;
+        for (int t = 1; t <= a.znd[28 * Y]; t++) {
+          if (a.znd[28 * Y + t] != pz) continue;
+          if (!have) {
+            kk = rigid_update(a, pk);
+            have = true;
+          }
+          float4 e;
+          float fm;
+          if (pair_force(P, kk, ki, e, fm)) F = f4add(F, f4mul(e, fm));
+        }
+      }
+    }
+    a.pf_new[pi] = F;
+    a.pf_new[pi + np] = make_float4(0.f, 0.f, 0.f, 0.f);
+    return;
+  }
+  if (pz >= 0 && pz < nzones) {
+    const int nn = a.znd[28 * pz];
+    for (int t = lane; t < nn; t += 32) {
+      const int zid = a.znd[28 * pz + 1 + t];
+      if (zid < 0 || zid >= nzones) continue;  // zone ids past the grid name no zone
+      const int cnt = a.numParInZone[zid];
+      for (int j = 0; j < cnt; j++) {
+        const int pj = a.zoneMembers[zid * np + j];
+        if (!(pi > pj)) continue;
+        const Kin kj = rigid_update(a, pj);
+        float4 e;
+        float fm;
+        if (pair_force(P, ki, kj, e, fm)) F = f4sub(F, f4mul(e, fm));
+      }
+    }
+    for (int r = a.revStart[pz] + lane; r < a.revStart[pz + 1]; r += 32) {
+      const int Y = a.revList[r];
+      const int cnt = a.numParInZone[Y];
+      for (int j = 0; j < cnt; j++) {
+        const int pk = a.zoneMembers[Y * np + j];
+        if (!(pk > pi)) continue;
+        const Kin kk = rigid_update(a, pk);
+        float4 e;
+        float fm;
+        if (pair_force(P, kk, ki, e, fm)) F = f4add(F, f4mul(e, fm));
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    F.x = __fadd_rn(F.x, __shfl_xor_sync(0xffffffffu, F.x, o));
+    F.y = __fadd_rn(F.y, __shfl_xor_sync(0xffffffffu, F.y, o));
+    F.z = __fadd_rn(F.z, __shfl_xor_sync(0xffffffffu, F.z, o));
+    F.w = __fadd_rn(F.w, __shfl_xor_sync(0xffffffffu, F.w, o));
+  }
+  if (lane != 0) return;
+  // z-wall repulsion (CPU_program.cl:174-182).
+  const float lo = __fsub_rn(P.zbuf, ki.x.z);
+  if (lo > 0) F.z = __fadd_rn(F.z, __fmul_rn(P.kcol, lo));
+  const float up = __fsub_rn(ki.x.z, __fsub_rn((float)P.Sint[2], P.zbuf));
+  if (up > 0) F.z = __fsub_rn(F.z, __fmul_rn(P.kcol, up));
+  a.pf_new[pi] = F;
+  a.pf_new[pi + np] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// update_particle_zones (CPU_program.cl:280-315) for all spheres: members of
+// each zone listed in increasing sphere index, the order the reference's
+// serial work-item loop produces.
+__global__ void zone_rebuild_kernel(const ZoneArgs a) {
+  const ParticleParams& P = a.p;
+  const int np = P.np;
+  const int nz = P.numZones[0] * P.numZones[1] * P.numZones[2];
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
+    const float4 x = a.kin[p];
+    int zx = (int)(x.x / P.zoneWidth[0]), zy = (int)(x.y / P.zoneWidth[1]), zz = (int)(x.z / P.zoneWidth[2]);
+    int zid = zx + P.numZones[0] * (zy + P.numZones[1] * zz);
+    if (zid < 0 || zid >= nz) {
+      atomicOr(a.err, ERR_ZONE_RANGE);
+      zid = zid < 0 ? 0 : nz - 1;
+    }
+    a.zoneOf[p] = zid;
+    a.parsZone[p] = zid;
+  }
+  __syncthreads();
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    int c = 0;
+    for (int p = 0; p < np; p++)
+      if (a.zoneOf[p] == z) a.zoneMembers[z * np + c++] = p;
+    a.numParInZone[z] = c;
+  }
+}
+
+__global__ void marker_cells_kernel(const float4* mrec, int M, int* cells) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  int x0, y0, z0;
+  decode_marker(mrec[2 * m], mrec[2 * m + 1], x0, y0, z0);
+  cells[3 * m] = x0;
+  cells[3 * m + 1] = y0;
+  cells[3 * m + 2] = z0;
+}
+
+// ---------------------------------------------------------------------------
+// Launchers.
+template <bool FIRST, bool VAR, int COLL>
+static cudaError_t launch_fluid_t(const FluidArgs& a, cudaStream_t s) {
+  dim3 block(TILE_X, TILE_Y, 2);
+  dim3 grid(a.g.ntx, a.g.nty, a.g.ntz);
+  fluid_step_kernel<FIRST, VAR, COLL><<<grid, block, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fluid(const FluidArgs& a, bool first, bool variable, int collision, cudaStream_t s) {
+  if (collision == 0) {
+    if (first) return variable ? launch_fluid_t<true, true, 0>(a, s) : launch_fluid_t<true, false, 0>(a, s);
+    return variable ? launch_fluid_t<false, true, 0>(a, s) : launch_fluid_t<false, false, 0>(a, s);
+  }
+  if (first) return variable ? launch_fluid_t<true, true, 1>(a, s) : launch_fluid_t<true, false, 1>(a, s);
+  return variable ? launch_fluid_t<false, true, 1>(a, s) : launch_fluid_t<false, false, 1>(a, s);
+}
+
+cudaError_t launch_materialize_f(const FluidArgs& a, float* out, cudaStream_t s) {
+  materialize_f_kernel<<<1184, 256, 0, s>>>(a, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s) {
+  const int ngroups = a.p.np * a.p.nfa;
+  const int threads = a.p.L < 128 ? 128 : a.p.L;
+  const int warps = threads / 32;
+  const int ppblocks = (a.p.np + warps - 1) / warps;
+  const size_t smem = sizeof(float4) * 2 * threads;
+  particle_step_kernel<<<ngroups + ppblocks, threads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zones(const ZoneArgs& a, cudaStream_t s) {
+  zone_rebuild_kernel<<<1, 1024, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spread_field(const Geom& g, const TileLists& t, int last_step, float* out, unsigned* err,
+                                cudaStream_t s) {
+  dim3 grid(g.ntx, g.nty, g.ntz);
+  spread_field_kernel<<<grid, 256, 0, s>>>(g, t, last_step, out, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_marker_cells(const float4* mrec, int M, int* cells, cudaStream_t s) {
+  marker_cells_kernel<<<(M + 255) / 256, 256, 0, s>>>(mrec, M, cells);
+  return cudaGetLastError();
+}
+
+}  // namespace d3q19

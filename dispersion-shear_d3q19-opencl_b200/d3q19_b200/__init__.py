@@ -1,0 +1,362 @@
+"""Python binding of the B200 D3Q19 LBM + IBM library (ctypes over the C ABI
+of include/d3q19_b200.h and the C host routines of host/d3q19_host.h).
+
+The GPU path runs only through lib/libd3q19_b200.so; if that library (or a
+usable sm_100 device) is missing, the calls raise -- there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(PKG, "lib")
+CUDA_LIB = os.path.join(LIBDIR, "libd3q19_b200.so")
+HOST_LIB = os.path.join(LIBDIR, "libd3q19_host.so")
+
+STATUS = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ENODEV", -5: "EOVERFLOW", -6: "ENUMERIC",
+          -7: "ESTATE"}
+
+_INT_FIELDS = [
+    ("MaxIterations", 1), ("BasisVel", 57), ("LatticeSize", 3), ("SystemSize", 3), ("BufferSize", 3),
+    ("BoundaryConds", 3), ("NumZones", 3), ("MaintainShear", 1), ("ViscosityModel", 1), ("NumParticles", 1),
+    ("ParForceModel", 1), ("MaxSurfPointsPerNode", 1), ("InterpOrderIBM", 1), ("PointsPerParticle", 1),
+    ("PointsPerWorkGroup", 1), ("TotalSurfPoints", 1), ("WorkGroupsPerParticle", 1)]
+_FLP_FIELDS = [
+    ("ConstBodyForce", 3), ("EqWeights", 19), ("VelUpper", 3), ("VelLower", 3), ("NewtonianTau", 1),
+    ("ViscosityParams", 4), ("ZoneWidth", 3), ("ParticleDiam", 1), ("ParticleMass", 1), ("PointArea", 1),
+    ("ParticleMomInertia", 1), ("ParForceParams", 2), ("ParticleZBuffer", 1), ("DirectForcingCoeff", 1)]
+
+
+def _fields(spec, ct):
+    return [(n, ct * k) if k > 1 else (n, ct) for n, k in spec]
+
+
+class IntParams(C.Structure):
+    """int_param_struct (struct_header_device.h:4-31)."""
+    _fields_ = _fields(_INT_FIELDS, C.c_int)
+
+
+class FlpParams(C.Structure):
+    """flp_param_struct (struct_header_device.h:34-57)."""
+    _fields_ = _fields(_FLP_FIELDS, C.c_float)
+
+
+class Options(C.Structure):
+    _fields_ = [("variable_viscosity", C.c_int), ("collision", C.c_int), ("storage", C.c_int),
+                ("particle_precision", C.c_int), ("fixed_particles", C.c_int), ("num_par_threads", C.c_int),
+                ("rebuild_freq", C.c_int), ("tangential_vel_bc", C.c_int * 3), ("tau_max", C.c_float),
+                ("tau_min", C.c_float), ("casson_reg", C.c_float), ("device", C.c_int),
+                ("ibm_tile_capacity", C.c_int), ("arithmetic", C.c_int)]
+
+
+class DeviceInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 256), ("sm_count", C.c_int), ("cc_major", C.c_int), ("cc_minor", C.c_int),
+                ("global_mem_bytes", C.c_size_t), ("kernel_work_group_size", C.c_int)]
+
+
+class HostParams(C.Structure):
+    _fields_ = [("ConsolePrintFreq", C.c_int), ("InitialDist", C.c_char * 128), ("InitialVel", C.c_float * 3),
+                ("InitialParticleDistribution", C.c_int), ("ParticleBuffer", C.c_float),
+                ("InterpOrderIBM", C.c_int), ("DomainDecomp", C.c_int * 3), ("ParticleDensity", C.c_float),
+                ("RebuildFreq", C.c_int), ("VideoFreq", C.c_int), ("FluidOutputSpacing", C.c_int),
+                ("TangentialVelBC", C.c_int * 3), ("ShearStressFreq", C.c_int), ("RandParticleShift", C.c_float),
+                ("UseConstantViscosity", C.c_int), ("PointsOverride", C.c_int), ("FixedParticles", C.c_int),
+                ("ParticleSeed", C.c_uint), ("MinParticleGap", C.c_float), ("TauMax", C.c_float),
+                ("TauMin", C.c_float), ("CassonReg", C.c_float), ("Collision", C.c_int), ("Storage", C.c_int),
+                ("ParticlePrecision", C.c_int)]
+
+
+class Config(C.Structure):
+    """d3q19h_config: the reference's two parameter blocks + host parameters."""
+    _fields_ = [("ip", IntParams), ("fp", FlpParams), ("hp", HostParams)]
+
+
+assert C.sizeof(IntParams) == 332 and C.sizeof(FlpParams) == 176
+
+_cuda = None
+_host = None
+
+
+class D3Q19Error(RuntimeError):
+    pass
+
+
+def cuda_lib():
+    """The CUDA library; raises when it is missing (no fallback)."""
+    global _cuda
+    if _cuda is None:
+        if not os.path.exists(CUDA_LIB):
+            raise D3Q19Error(f"{CUDA_LIB} is not built (run build.py); there is no CPU path")
+        lib = C.CDLL(CUDA_LIB)
+        P = C.c_void_p
+        lib.d3q19_create.argtypes = [C.POINTER(IntParams), C.POINTER(FlpParams), C.POINTER(Options),
+                                     C.POINTER(C.c_void_p)]
+        lib.d3q19_last_error.restype = C.c_char_p
+        lib.d3q19_last_error.argtypes = [P]
+        lib.d3q19_tau_clamp_count.restype = C.c_longlong
+        lib.d3q19_tau_clamp_count.argtypes = [P]
+        lib.d3q19_stream.restype = P
+        lib.d3q19_stream.argtypes = [P]
+        lib.d3q19_periodic_map.argtypes = [C.POINTER(IntParams), P, C.c_int]
+        for name in ("d3q19_write_lattice", "d3q19_write_particles", "d3q19_write_zones", "d3q19_read_u",
+                     "d3q19_read_tau", "d3q19_read_parkin", "d3q19_read_parforce", "d3q19_read_parfluidforce",
+                     "d3q19_read_f", "d3q19_read_spread_force", "d3q19_read_marker_cells", "d3q19_read_zones",
+                     "d3q19_synchronize", "d3q19_destroy", "d3q19_write_periodic_map"):
+            getattr(lib, name).restype = C.c_int
+        lib.d3q19_step.argtypes = [P, C.c_int]
+        lib.d3q19_profile.argtypes = [P, C.c_int]
+        lib.d3q19_profile_read.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                           C.POINTER(C.c_int)]
+        lib.d3q19_run.argtypes = [P, C.c_int, C.c_int]
+        lib.d3q19_write_periodic_map.argtypes = [P, P, C.c_int]
+        _cuda = lib
+    return _cuda
+
+
+def host_lib():
+    global _host
+    if _host is None:
+        if not os.path.exists(HOST_LIB):
+            raise D3Q19Error(f"{HOST_LIB} is not built (run build.py)")
+        lib = C.CDLL(HOST_LIB)
+        lib.d3q19h_parse_text.argtypes = [C.c_char_p, C.POINTER(Config)]
+        lib.d3q19h_sphere_discretization.argtypes = [C.POINTER(Config), C.c_char_p, C.POINTER(C.POINTER(C.c_float))]
+        lib.d3q19h_eqsp_points.argtypes = [C.c_int, C.c_void_p]
+        lib.d3q19h_work_groups.argtypes = [C.POINTER(Config), C.c_int]
+        lib.d3q19h_init_lattice.argtypes = [C.POINTER(Config), C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.d3q19h_init_particles.argtypes = [C.POINTER(Config), C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.d3q19h_zone_grid.argtypes = [C.POINTER(Config)]
+        lib.d3q19h_zone_count.argtypes = [C.POINTER(Config)]
+        lib.d3q19h_init_zones.argtypes = [C.POINTER(Config)] + [C.c_void_p] * 7
+        lib.d3q19h_options.argtypes = [C.POINTER(Config), C.POINTER(Options)]
+        lib.d3q19h_compute_shear_stress.argtypes = [C.c_void_p, C.POINTER(Config), C.c_void_p, C.c_char_p]
+        lib.d3q19h_write_lattice_field.argtypes = [C.POINTER(Config), C.c_void_p, C.c_char_p, C.c_char_p]
+        lib.d3q19h_check.argtypes = [C.POINTER(Config)]
+        _host = lib
+    return _host
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _fmt(v):
+    if isinstance(v, (list, tuple)):
+        return " ".join(str(x) for x in v)
+    return str(v)
+
+
+def keywords_text(keywords: dict) -> str:
+    return "".join(f"{k:<32s}{_fmt(v)}\n" for k, v in keywords.items())
+
+
+def parse_config(text: str) -> Config:
+    cfg = Config()
+    host_lib().d3q19h_parse_text(text.encode(), C.byref(cfg))
+    return cfg
+
+
+def device_info(device: int = 0) -> DeviceInfo:
+    di = DeviceInfo()
+    rc = cuda_lib().d3q19_get_device_info(device, C.byref(di))
+    if rc:
+        raise D3Q19Error(f"d3q19_get_device_info: {STATUS.get(rc, rc)}: {cuda_lib().d3q19_last_error(None)!r}")
+    return di
+
+
+def periodic_map(ip: IntParams) -> np.ndarray:
+    lib = cuda_lib()
+    n = lib.d3q19_periodic_map(C.byref(ip), None, 0)
+    out = np.zeros(2 * max(n, 1), np.int32)
+    lib.d3q19_periodic_map(C.byref(ip), _ptr(out), out.size)
+    return out[: 2 * n]
+
+
+def eqsp_points(n: int) -> np.ndarray:
+    out = np.zeros(3 * n, np.float64)
+    host_lib().d3q19h_eqsp_points(n, _ptr(out))
+    return out.reshape(n, 3)
+
+
+class HostState:
+    """The initial state the reference's host builds (D3Q19-OpenCL.c host
+    routines, in sim_main.c's order), computed by the C host library."""
+
+    def __init__(self, cfg: Config, data_dir: str = ".", kernel_work_group_size: int = 256):
+        h = host_lib()
+        self.cfg = cfg
+        if h.d3q19h_check(C.byref(cfg)):
+            raise D3Q19Error("parameter check failed")
+        pts = C.POINTER(C.c_float)()
+        if h.d3q19h_sphere_discretization(C.byref(cfg), data_dir.encode(), C.byref(pts)) != 0:
+            raise D3Q19Error("malformed sphere discretisation file")
+        P = cfg.ip.PointsPerParticle
+        self.spherePoints = np.ctypeslib.as_array(pts, shape=(4 * P,)).copy()
+        C.CDLL(None).free(pts)
+        h.d3q19h_work_groups(C.byref(cfg), kernel_work_group_size)
+        ip = cfg.ip
+        nc = ip.LatticeSize[0] * ip.LatticeSize[1] * ip.LatticeSize[2]
+        self.f = np.zeros(19 * nc, np.float32)
+        self.u = np.zeros(3 * nc, np.float32)
+        self.tau = np.zeros(nc, np.float32)
+        if h.d3q19h_init_lattice(C.byref(cfg), _ptr(self.f), _ptr(self.u), _ptr(self.tau)):
+            raise D3Q19Error("lattice initialisation failed")
+        np_ = ip.NumParticles
+        nfa = max(ip.WorkGroupsPerParticle, 1)
+        self.parKin = np.zeros(16 * max(np_, 2), np.float32)
+        self.parForce = np.zeros(8 * max(np_, 1), np.float32)
+        self.parFluidForce = np.zeros(8 * max(np_, 1) * nfa, np.float32)
+        if h.d3q19h_init_particles(C.byref(cfg), _ptr(self.parKin), _ptr(self.parForce), _ptr(self.parFluidForce)):
+            raise D3Q19Error("particle initialisation failed")
+        self.parKin = self.parKin[: 16 * np_]
+        self.parForce = self.parForce[: 8 * np_]
+        self.parFluidForce = self.parFluidForce[: 8 * np_ * nfa]
+        h.d3q19h_zone_grid(C.byref(cfg))
+        Z = h.d3q19h_zone_count(C.byref(cfg))
+        nth = cfg.hp.DomainDecomp[0] * cfg.hp.DomainDecomp[1] * cfg.hp.DomainDecomp[2]
+        self.parsZone = np.zeros(max(np_, 1), np.int32)
+        self.zoneMembers = np.zeros(Z * max(np_, 1), np.int32)
+        self.numParInZone = np.zeros(Z, np.int32)
+        self.threadMembers = np.zeros(max(nth, 1) * max(np_, 1), np.int32)
+        self.numParInThread = np.zeros(max(nth, 1), np.int32)
+        self.zoneNeighDat = np.zeros(28 * Z, np.int32)
+        if np_ > 0 and h.d3q19h_init_zones(C.byref(cfg), _ptr(self.parKin), _ptr(self.parsZone),
+                                           _ptr(self.zoneMembers), _ptr(self.numParInZone),
+                                           _ptr(self.threadMembers), _ptr(self.numParInThread),
+                                           _ptr(self.zoneNeighDat)):
+            raise D3Q19Error("Particle out of bounds at zone initialization")
+        self.options = Options()
+        h.d3q19h_options(C.byref(cfg), C.byref(self.options))
+
+
+class Simulation:
+    """One GPU context: the reference's buffers resident on the device,
+    advanced step by step in the reference's kernel order."""
+
+    def __init__(self, ip: IntParams, fp: FlpParams, options: Options | None = None):
+        self.lib = cuda_lib()
+        self.ip = IntParams.from_buffer_copy(bytes(ip))
+        self.fp = FlpParams.from_buffer_copy(bytes(fp))
+        self.options = options or Options()
+        h = C.c_void_p()
+        rc = self.lib.d3q19_create(C.byref(self.ip), C.byref(self.fp), C.byref(self.options), C.byref(h))
+        if rc:
+            raise D3Q19Error(f"d3q19_create: {STATUS.get(rc, rc)}: {self.lib.d3q19_last_error(None).decode()}")
+        self.h = h
+        self.nc = self.ip.LatticeSize[0] * self.ip.LatticeSize[1] * self.ip.LatticeSize[2]
+        self.np = self.ip.NumParticles
+        self.nfa = max(self.ip.WorkGroupsPerParticle, 1)
+        self.nzones = self.ip.NumZones[0] * self.ip.NumZones[1] * self.ip.NumZones[2]
+
+    @classmethod
+    def from_host_state(cls, hs: HostState, **option_overrides):
+        opt = Options.from_buffer_copy(bytes(hs.options))
+        for k, v in option_overrides.items():
+            setattr(opt, k, v)
+        sim = cls(hs.cfg.ip, hs.cfg.fp, opt)
+        sim.write_lattice(hs.f, hs.u, hs.tau)
+        sim.write_periodic_map(periodic_map(hs.cfg.ip))
+        if sim.np > 0:
+            sim.write_particles(hs.parKin, hs.parForce, hs.parFluidForce, hs.spherePoints)
+            sim.write_zones(hs.zoneNeighDat, hs.parsZone, hs.zoneMembers, hs.numParInZone, hs.threadMembers,
+                            hs.numParInThread)
+        return sim
+
+    def _check(self, rc, what):
+        if rc:
+            raise D3Q19Error(f"{what}: {STATUS.get(rc, rc)}: {self.lib.d3q19_last_error(self.h).decode()}")
+
+    def write_lattice(self, f, u, tau=None):
+        f = np.ascontiguousarray(f, np.float32)
+        u = np.ascontiguousarray(u, np.float32)
+        tau = None if tau is None else np.ascontiguousarray(tau, np.float32)
+        self._check(self.lib.d3q19_write_lattice(self.h, _ptr(f), _ptr(u), _ptr(tau)), "write_lattice")
+
+    def write_particles(self, parKin, parForce, parFluidForce, spherePoints):
+        a = [np.ascontiguousarray(x, np.float32) for x in (parKin, parForce, parFluidForce, spherePoints)]
+        self._check(self.lib.d3q19_write_particles(self.h, *[_ptr(x) for x in a]), "write_particles")
+
+    def write_zones(self, znd, parsZone, zoneMembers, numParInZone, threadMembers=None, numParInThread=None):
+        a = [None if x is None else np.ascontiguousarray(x, np.int32)
+             for x in (znd, parsZone, zoneMembers, numParInZone, threadMembers, numParInThread)]
+        self._check(self.lib.d3q19_write_zones(self.h, *[_ptr(x) for x in a]), "write_zones")
+
+    def write_periodic_map(self, strMap):
+        s = np.ascontiguousarray(strMap, np.int32)
+        self._check(self.lib.d3q19_write_periodic_map(self.h, _ptr(s), len(s) // 2), "write_periodic_map")
+
+    def step(self, t: int):
+        self._check(self.lib.d3q19_step(self.h, t), "step")
+
+    def run(self, t0: int, n: int):
+        self._check(self.lib.d3q19_run(self.h, t0, n), "run")
+
+    def synchronize(self):
+        self._check(self.lib.d3q19_synchronize(self.h), "synchronize")
+
+    def _read(self, fn, n, dtype=np.float32):
+        out = np.zeros(n, dtype)
+        self._check(getattr(self.lib, fn)(self.h, _ptr(out)), fn)
+        return out
+
+    def read_u(self):
+        return self._read("d3q19_read_u", 3 * self.nc)
+
+    def read_tau(self):
+        return self._read("d3q19_read_tau", self.nc)
+
+    def read_f(self):
+        return self._read("d3q19_read_f", 19 * self.nc)
+
+    def read_parkin(self):
+        return self._read("d3q19_read_parkin", 16 * self.np)
+
+    def read_parforce(self):
+        return self._read("d3q19_read_parforce", 8 * self.np)
+
+    def read_parfluidforce(self):
+        return self._read("d3q19_read_parfluidforce", 8 * self.np * self.nfa)
+
+    def read_spread_force(self):
+        return self._read("d3q19_read_spread_force", 3 * self.nc)
+
+    def read_marker_cells(self):
+        return self._read("d3q19_read_marker_cells", 3 * self.np * self.ip.PointsPerParticle, np.int32)
+
+    def read_zones(self):
+        pz = np.zeros(self.np, np.int32)
+        zm = np.zeros(self.nzones * self.np, np.int32)
+        nz = np.zeros(self.nzones, np.int32)
+        self._check(self.lib.d3q19_read_zones(self.h, _ptr(pz), _ptr(zm), _ptr(nz)), "read_zones")
+        return pz, zm, nz
+
+    def profile(self, enable: bool):
+        self._check(self.lib.d3q19_profile(self.h, int(enable)), "profile")
+
+    def profile_read(self):
+        a, b = C.c_double(), C.c_double()
+        na, nb = C.c_int(), C.c_int()
+        self._check(self.lib.d3q19_profile_read(self.h, C.byref(a), C.byref(na), C.byref(b), C.byref(nb)),
+                    "profile_read")
+        return a.value, na.value, b.value, nb.value
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self.lib.d3q19_stream(self.h) or 0)
+
+    def tau_clamp_count(self) -> int:
+        return int(self.lib.d3q19_tau_clamp_count(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.d3q19_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,241 @@
+/* d3q19_b200.h -- C ABI of the B200 (sm_100a) implementation of the D3Q19
+ * lattice-Boltzmann + immersed-boundary sphere-suspension time step of
+ * SB8/Dispersion-Shear_D3Q19-OpenCL.
+ *
+ * The library replaces the reference's OpenCL host API calls and kernel
+ * contract (sim_main.c:15-527, D3Q19-OpenCL.c:465-556, 847-971): plain
+ * pointers and sizes, host buffers owned by the caller, device memory and one
+ * CUDA stream owned by the context.  Every entry point returns 0 on success
+ * or a negative d3q19_status; no entry point exits the process (the
+ * reference's error_check() calls exit(0), D3Q19-OpenCL.c:1169-1246).
+ *
+ * Array layouts are the reference's (GPU_program.cl:316-350, 81-90):
+ *   f       float[19][N_C]        q-major, x fastest, N_C = Lx*Ly*Lz incl. buffer
+ *   u       float[3][N_C]
+ *   tau_lb  float[N_C]
+ *   parKin  float4[4*np]          position, velocity, quaternion, angular velocity
+ *   parForce float4[2*np]         force, torque
+ *   parFluidForce float4[2*np*nfa]  per work-group force partials, then torques
+ *   spherePoints float4[P]        unit-sphere points scaled by the radius
+ */
+#ifndef D3Q19_B200_H
+#define D3Q19_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Parameter blocks, byte-for-byte the layout of struct_header_device.h:4-57
+ * (332 and 176 bytes); the reference uploads them raw (sim_main.c:204-205). */
+typedef struct {
+  int MaxIterations;
+  int BasisVel[19][3];
+  int LatticeSize[3];
+  int SystemSize[3];
+  int BufferSize[3];
+  int BoundaryConds[3];
+  int NumZones[3];
+  int MaintainShear;
+  int ViscosityModel;
+  int NumParticles;
+  int ParForceModel;
+  int MaxSurfPointsPerNode;
+  int InterpOrderIBM;
+  int PointsPerParticle;
+  int PointsPerWorkGroup;
+  int TotalSurfPoints;
+  int WorkGroupsPerParticle;
+} int_param_struct;
+
+typedef struct {
+  float ConstBodyForce[3];
+  float EqWeights[19];
+  float VelUpper[3];
+  float VelLower[3];
+  float NewtonianTau;
+  float ViscosityParams[4];
+  float ZoneWidth[3];
+  float ParticleDiam;
+  float ParticleMass;
+  float PointArea;
+  float ParticleMomInertia;
+  float ParForceParams[2];
+  float ParticleZBuffer;
+  float DirectForcingCoeff;
+} flp_param_struct;
+
+enum d3q19_status {
+  D3Q19_OK = 0,
+  D3Q19_EINVAL = -1,    /* bad argument or unsupported parameter combination */
+  D3Q19_ENOMEM = -2,    /* device allocation failed */
+  D3Q19_ECUDA = -3,     /* CUDA runtime error (see d3q19_last_error) */
+  D3Q19_ENODEV = -4,    /* no usable sm_100 device */
+  D3Q19_EOVERFLOW = -5, /* a lattice tile received more IBM markers than its list holds */
+  D3Q19_ENUMERIC = -6,  /* non-finite density or velocity detected on the device */
+  D3Q19_ESTATE = -7     /* call out of order (e.g. step before the lattice is written) */
+};
+
+/* Options with no counterpart in the reference's parameter structs.  A
+ * zero-initialised struct reproduces the reference as shipped. */
+typedef struct {
+  /* 0: GPU_program.cl as shipped (USE_CONSTANT_VISCOSITY defined, tau =
+   * NewtonianTau).  1: the reference's other build, without that define
+   * (GPU_program.cl:457-564): local tau from the strain rate (power-law,
+   * Casson, Herschel-Bulkley via ViscosityModel). */
+  int variable_viscosity;
+  /* 0: the reference's MRT rates (GPU_program.cl:453, 567-568).
+   * 1: BGK, every rate 1/tau (GPU_program.cl:867-947 generalised). */
+  int collision;
+  /* 0: FP32 distributions (reference).  1: FP16, 2: BF16 storage of
+   * f_i - w_i with FP32 arithmetic. */
+  int storage;
+  /* 0: FP32 particle state and sums in the reference's order.
+   * 1: FP64 per-sphere force/torque sums and Newton-Euler integration. */
+  int particle_precision;
+  /* 1: spheres keep their initial position and velocity (forces are still
+   * computed and reported). */
+  int fixed_particles;
+  /* Particle work split of the reference's CPU device (numParThreads =
+   * product of domain_decomposition, sim_main.c:65); used to interpret
+   * threadMembers/numParInThread. */
+  int num_par_threads;
+  /* Zone lists are rebuilt after steps with t % rebuild_freq == 0
+   * (rebuild_neigh_list_freq, sim_main.c:429). */
+  int rebuild_freq;
+  /* Experimental tangential velocity boundaries (tangential_vel_bcs,
+   * sim_main.c:388-402). */
+  int tangential_vel_bc[3];
+  /* Upper clamp of the local tau (0 = none, as the reference). */
+  float tau_max;
+  /* Lower clamp of the local tau (0 = the reference's MIN_TAU 0.505,
+   * GPU_program.cl:6). */
+  float tau_min;
+  /* Casson regularisation: shear rate floor added in quadrature (0 = none). */
+  float casson_reg;
+  /* CUDA device ordinal. */
+  int device;
+  /* Markers per lattice tile list (0 = automatic). */
+  int ibm_tile_capacity;
+  /* 0: fast arithmetic (one forward and one inverse moment transform,
+   * contraction allowed, integer fixed-point spreading).  1: the reference's
+   * floating-point evaluation order (both transforms as written, no
+   * contraction, slot-ordered spreading, contact forces summed in the
+   * reference's order): the reference's results bit for bit from the same
+   * state, except where a pow() of the viscosity law rounds differently. */
+  int arithmetic;
+} d3q19_options;
+
+typedef struct {
+  char name[256];
+  int sm_count;
+  int cc_major, cc_minor;
+  size_t global_mem_bytes;
+  /* Work-group size the IBM kernel reports; the host derives
+   * PointsPerWorkGroup = min(pow2 >= this, PointsPerParticle) from it as the
+   * reference does with CL_KERNEL_WORK_GROUP_SIZE (D3Q19-OpenCL.c:536-550). */
+  int kernel_work_group_size;
+} d3q19_device_info;
+
+typedef struct d3q19_ctx d3q19_ctx;
+
+/* Replaces analyse_platform (D3Q19-OpenCL.c:847-971) and the
+ * clGetKernelWorkGroupInfo query (D3Q19-OpenCL.c:536-538). */
+int d3q19_get_device_info(int device, d3q19_device_info* out);
+
+/* Replaces clCreateContext / clCreateCommandQueue / program build /
+ * clCreateKernel / clCreateBuffer (sim_main.c:15-42, 115-190;
+ * D3Q19-OpenCL.c:465-556).  Copies both parameter blocks. */
+int d3q19_create(const int_param_struct* ip, const flp_param_struct* fp, const d3q19_options* opt,
+                 d3q19_ctx** out);
+
+/* Replaces clEnqueueWriteBuffer of fA/fB/u/tau_lb (sim_main.c:193-198).
+ * f is the state the next step reads (both reference buffers start equal);
+ * tau_lb may be NULL (filled with NewtonianTau, D3Q19-OpenCL.c:179). */
+int d3q19_write_lattice(d3q19_ctx* ctx, const float* f, const float* u, const float* tau_lb);
+
+/* Replaces the particle buffer uploads (sim_main.c:140-150, 189, 202). */
+int d3q19_write_particles(d3q19_ctx* ctx, const float* parKin, const float* parForce, const float* parFluidForce,
+                          const float* spherePoints);
+
+/* Replaces the zone buffer uploads (sim_main.c:152-177).  zoneNeighDat is
+ * int[28*zones], zoneMembers int[zones*np], threadMembers
+ * int[num_par_threads*np]. */
+int d3q19_write_zones(d3q19_ctx* ctx, const int* zoneNeighDat, const int* parsZone, const int* zoneMembers,
+                      const int* numParInZone, const int* threadMembers, const int* numParInThread);
+
+/* Builds the periodic boundary node list of create_periodic_stream_mapping
+ * (D3Q19-OpenCL.c:973-1112) into strMap = [indices..., types...] (capacity
+ * ints); returns the node count (strMap may be NULL to query it).  Host
+ * only, needs no GPU. */
+int d3q19_periodic_map(const int_param_struct* ip, int* strMap, int capacity);
+
+/* Replaces the strMap upload (sim_main.c:186, 203).  The periodic copy is
+ * fused into the streaming gather, so the map is checked against the one the
+ * boundary conditions imply (D3Q19-OpenCL.c:973-1112); a mismatch is
+ * D3Q19_EINVAL. */
+int d3q19_write_periodic_map(d3q19_ctx* ctx, const int* strMap, int numPeriodicNodes);
+
+/* One time step t (t >= 1) with the order and data dependencies of
+ * sim_main.c:324-447: collide-stream with the force spread at step t-1, the
+ * periodic and velocity boundaries, the rigid-body update from the forces of
+ * step t-1, IBM interpolation of u(t) at the moved markers and spreading,
+ * particle-particle forces, and the zone rebuild when t % rebuild_freq == 0.
+ * Asynchronous on the context's stream. */
+int d3q19_step(d3q19_ctx* ctx, int t);
+
+/* Steps t0 .. t0+nsteps-1, replayed from captured CUDA graphs. */
+int d3q19_run(d3q19_ctx* ctx, int t0, int nsteps);
+
+/* clFinish (sim_main.c:407, 447): waits for the stream and reports device
+ * errors (tile overflow, non-finite values). */
+int d3q19_synchronize(d3q19_ctx* ctx);
+
+/* Read-backs (sim_main.c:452-462, 478, 486).  Synchronous. */
+int d3q19_read_u(d3q19_ctx* ctx, float* u);
+int d3q19_read_tau(d3q19_ctx* ctx, float* tau_lb);
+int d3q19_read_parkin(d3q19_ctx* ctx, float* parKin);
+int d3q19_read_parforce(d3q19_ctx* ctx, float* parForce);
+int d3q19_read_parfluidforce(d3q19_ctx* ctx, float* parFluidForce);
+/* The distribution buffer the last step wrote, as the reference holds it
+ * after the boundary kernels (interior nodes; buffer-layer nodes are 0). */
+int d3q19_read_f(d3q19_ctx* ctx, float* f);
+/* The spread IBM force field of the last step, as the reference's gpf slot 0
+ * after sum_particle_fluid_forces (GPU_program.cl:258-289): float[3][N_C]. */
+int d3q19_read_spread_force(d3q19_ctx* ctx, float* gpf0);
+/* Corner cell (x_i0, y_i0, z_i0) of every marker of the last step
+ * (GPU_program.cl:150-156): int[3*TotalSurfPoints]. */
+int d3q19_read_marker_cells(d3q19_ctx* ctx, int* cells);
+/* Zone lists after the last rebuild (update_particle_zones). */
+int d3q19_read_zones(d3q19_ctx* ctx, int* parsZone, int* zoneMembers, int* numParInZone);
+
+/* Number of lattice nodes whose local tau was clamped to 0.505 since the
+ * context was created (the reference prints a device warning instead,
+ * GPU_program.cl:1071-1074). */
+long long d3q19_tau_clamp_count(d3q19_ctx* ctx);
+
+/* Kernel timing: with enable = 1 the following steps launch eagerly (no graph
+ * replay) with CUDA events around every collide-stream and particle launch;
+ * enable = 0 stops.  d3q19_profile_read synchronises and returns the summed
+ * device time in ms and the launch counts since profiling was enabled.
+ * No counterpart in the reference (it has no timers). */
+int d3q19_profile(d3q19_ctx* ctx, int enable);
+int d3q19_profile_read(d3q19_ctx* ctx, double* fluid_ms, int* fluid_launches, double* particle_ms,
+                       int* particle_launches);
+
+/* The context's CUDA stream (cudaStream_t) for callers that order their own
+ * work after the step. */
+void* d3q19_stream(d3q19_ctx* ctx);
+
+/* Text of the last error on this context (or of the last failed create when
+ * ctx is NULL). */
+const char* d3q19_last_error(d3q19_ctx* ctx);
+
+/* Replaces clRelease* (sim_main.c:503-525). */
+int d3q19_destroy(d3q19_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

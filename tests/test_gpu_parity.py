@@ -1,0 +1,159 @@
+"""Parity of the CUDA path (through the C ABI) with the reference itself.
+
+Golden vectors: the reference's own host program and OpenCL kernels run on
+the host (tests/golden/make_golden.py), from which the GPU starts.
+
+* arithmetic = 1 (reference-exact) must reproduce the reference's state
+  after N steps bit for bit: test_reference_exact_arithmetic_bitwise.
+* arithmetic = 0 (the fast path: re-associated moment algebra, contraction,
+  integer fixed-point spreading) is held to a relative L2 of 1e-5, except for
+  observables the reference itself cannot reproduce to that level under a
+  benign change of arithmetic: compiled with fused multiply-add contraction
+  (what an OpenCL GPU compiler does by default) the reference moves by the
+  amounts in golden/rounding_spread.json, and there the bound is ten times
+  that spread.  Sphere velocities and forces after a few steps are residuals
+  of nearly cancelling marker forces; they are compared in units of the
+  problem's own scale (wall speed, summed marker force) rather than of their
+  near-zero values.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from cases import CASES, is_variable
+from gpu_helpers import REL_TOL, interior_mask, rel_l2, sim_from_golden
+
+pytestmark = pytest.mark.gpu
+
+with open(os.path.join(os.path.dirname(__file__), "golden", "rounding_spread.json")) as _fh:
+    SPREAD = json.load(_fh)
+
+
+def bound(name, key):
+    return max(REL_TOL, 10.0 * SPREAD[name].get(key, 0.0))
+
+
+def scaled_err(a, b, scale):
+    """L2 error relative to max(|b|, a scale per entry)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), scale * np.sqrt(b.size)))
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_fast_arithmetic_matches_reference(name):
+    case = CASES[name]
+    g = load_golden(name)
+    sim, ip, fp = sim_from_golden(g, case)
+    n = int(g["iterations"])
+    sim.run(1, n)
+    sim.synchronize()
+    mu = interior_mask(ip, 3)
+    u = sim.read_u()
+    assert rel_l2(u[mu], g["final_u"][mu]) <= bound(name, "u")
+    if "final_f" in g:
+        mf = interior_mask(ip, 19)
+        assert rel_l2(sim.read_f()[mf], g["final_f"][mf]) <= REL_TOL
+    if is_variable(case):
+        m1 = interior_mask(ip, 1)
+        assert rel_l2(sim.read_tau()[m1], g["final_tau_lb"][m1]) <= bound(name, "tau")
+    if ip.NumParticles > 0:
+        np_ = ip.NumParticles
+        U = max(abs(v) for v in list(fp.VelUpper) + list(fp.VelLower) + [1e-3])
+        Fscale = fp.PointArea * ip.PointsPerParticle * U  # summed marker force at slip U
+        kin = sim.read_parkin().reshape(4 * np_, 4)
+        ref = g["final_parKin"].reshape(4 * np_, 4)
+        assert rel_l2(kin[:np_, :3], ref[:np_, :3]) <= REL_TOL  # positions
+        assert scaled_err(kin[np_:2 * np_, :3], ref[np_:2 * np_, :3], U) <= REL_TOL  # velocities
+        R = fp.ParticleDiam / 2
+        assert scaled_err(kin[3 * np_:, :3], ref[3 * np_:, :3], U / R) <= REL_TOL  # angular velocities
+        pff = sim.read_parfluidforce().reshape(-1, 4)
+        rpff = g["final_parFluidForce"].reshape(-1, 4)
+        half = pff.shape[0] // 2
+        assert scaled_err(pff[:half, :3], rpff[:half, :3], Fscale / ip.WorkGroupsPerParticle) <= REL_TOL
+        assert scaled_err(pff[half:, :3], rpff[half:, :3], Fscale * R / ip.WorkGroupsPerParticle) <= REL_TOL
+        pf = sim.read_parforce().reshape(-1, 4)
+        rpf = g["final_parForce"].reshape(-1, 4)
+        assert scaled_err(pf[:np_, :3], rpf[:np_, :3], Fscale) <= REL_TOL
+        gpf = sim.read_spread_force()
+        assert rel_l2(gpf[mu], g["final_gpf0"][mu]) <= bound(name, "gpf0")
+        pz, zm, nz = sim.read_zones()
+        assert np.array_equal(pz, g["final_parsZone"])
+        assert np.array_equal(nz, g["final_numParInZone"])
+        valid = g["final_zoneMembers"] >= 0
+        assert np.array_equal(zm[valid], g["final_zoneMembers"][valid])
+    sim.close()
+
+
+def test_graph_replay_matches_eager_steps():
+    """d3q19_run (CUDA-graph chunks) and d3q19_step give the same state."""
+    case = CASES["contacts"]
+    g = load_golden("contacts")
+    a, ip, _ = sim_from_golden(g, case)
+    b, _, _ = sim_from_golden(g, case)
+    n = 150
+    a.run(1, n)
+    for t in range(1, n + 1):
+        b.step(t)
+    for rd in ("read_u", "read_parkin", "read_parfluidforce", "read_parforce"):
+        x, y = getattr(a, rd)(), getattr(b, rd)()
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), rd
+    a.close()
+    b.close()
+
+
+# Cases whose viscosity law evaluates pow() with an exponent other than 0.5,
+# 1 or 2: pow is not correctly rounded in glibc (which the golden vectors
+# used) nor on the GPU, so the last bit of tau can differ at a few nodes and
+# the strain-rate feedback carries that on; everything else is bit-exact.
+POW_CASES = {"power_law", "herschel_bulkley", "power_law_sphere"}
+
+
+def _assert_bitwise(x, y, what):
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    same = x.view(np.uint32) == y.view(np.uint32)
+    assert same.all(), f"{what}: {np.count_nonzero(~same)} of {same.size} differ, rel-L2 {rel_l2(x, y):.2e}"
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_reference_exact_arithmetic_bitwise(name):
+    """arithmetic = 1 reproduces the reference's own state after N steps bit
+    for bit (velocity, distributions, tau, sphere kinematics, force partials,
+    contact forces, spread force field, zone lists)."""
+    case = CASES[name]
+    g = load_golden(name)
+    sim, ip, fp = sim_from_golden(g, case, arithmetic=1)
+    n = int(g["iterations"])
+    sim.run(1, n)
+    sim.synchronize()
+    mu = interior_mask(ip, 3)
+    got = {"u": sim.read_u()[mu]}
+    ref = {"u": g["final_u"][mu]}
+    if "final_f" in g:
+        mf = interior_mask(ip, 19)
+        got["f"], ref["f"] = sim.read_f()[mf], g["final_f"][mf]
+    if is_variable(case):
+        m1 = interior_mask(ip, 1)
+        got["tau"], ref["tau"] = sim.read_tau()[m1], g["final_tau_lb"][m1]
+    if ip.NumParticles > 0:
+        got["parKin"], ref["parKin"] = sim.read_parkin(), g["final_parKin"]
+        got["parFluidForce"], ref["parFluidForce"] = sim.read_parfluidforce(), g["final_parFluidForce"]
+        got["parForce"], ref["parForce"] = sim.read_parforce(), g["final_parForce"]
+        got["gpf0"], ref["gpf0"] = sim.read_spread_force()[mu], g["final_gpf0"][mu]
+        pz, zm, nz = sim.read_zones()
+        assert np.array_equal(pz, g["final_parsZone"])
+        assert np.array_equal(nz, g["final_numParInZone"])
+        valid = g["final_zoneMembers"] >= 0
+        assert np.array_equal(zm[valid], g["final_zoneMembers"][valid])
+    sim.close()
+    if name in POW_CASES:
+        for k in ("u", "tau"):
+            if k in got:
+                assert rel_l2(got[k], ref[k]) <= bound(name, k), k
+        return
+    for k in got:
+        _assert_bitwise(got[k], ref[k], k)
