@@ -66,7 +66,7 @@ class HostParams(C.Structure):
                 ("UseConstantViscosity", C.c_int), ("PointsOverride", C.c_int), ("FixedParticles", C.c_int),
                 ("ParticleSeed", C.c_uint), ("MinParticleGap", C.c_float), ("TauMax", C.c_float),
                 ("TauMin", C.c_float), ("CassonReg", C.c_float), ("Collision", C.c_int), ("Storage", C.c_int),
-                ("ParticlePrecision", C.c_int)]
+                ("ParticlePrecision", C.c_int), ("Arithmetic", C.c_int)]
 
 
 class Config(C.Structure):

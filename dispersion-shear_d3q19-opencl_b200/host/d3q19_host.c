@@ -80,6 +80,7 @@ static const keyword_t KEYWORDS[] = {
     {"lbm_collision", T_INT, HPO(Collision), "0"},
     {"storage_precision", T_INT, HPO(Storage), "0"},
     {"particle_precision", T_INT, HPO(ParticlePrecision), "0"},
+    {"reference_arithmetic", T_INT, HPO(Arithmetic), "0"},
 };
 #define NKEYWORDS ((int)(sizeof(KEYWORDS) / sizeof(KEYWORDS[0])))
 
@@ -707,5 +708,6 @@ void d3q19h_options(const d3q19h_config* cfg, d3q19_options* o) {
   for (int d = 0; d < 3; d++) o->tangential_vel_bc[d] = cfg->hp.TangentialVelBC[d];
   o->tau_max = cfg->hp.TauMax;
   o->tau_min = cfg->hp.TauMin;
+  o->arithmetic = cfg->hp.Arithmetic;
   o->casson_reg = cfg->hp.CassonReg;
 }

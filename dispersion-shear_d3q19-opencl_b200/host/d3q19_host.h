@@ -48,6 +48,7 @@ typedef struct {
   int Collision;              /* lbm_collision: 0 MRT (reference), 1 BGK */
   int Storage;                /* storage_precision: 0 fp32, 1 fp16 shifted, 2 bf16 shifted */
   int ParticlePrecision;      /* particle_precision: 0 fp32 (reference), 1 fp64 */
+  int Arithmetic;             /* reference_arithmetic: 1 = the reference's evaluation order */
 } d3q19h_host_params;
 
 typedef struct {
