@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <tuple>
 #include <vector>
 
@@ -785,4 +786,80 @@ extern "C" int d3q19_destroy(d3q19_ctx* c) {
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
+}
+
+/* ---------------------------------------------------------------------------
+ * Spread force field read-back that allocates nothing.
+ *
+ * d3q19_read_spread_force builds the 3*N_C-float field in the context's
+ * scratch buffer, which it grows with cudaFree + cudaMalloc when a larger
+ * read-back comes along.  Two kinds of caller cannot accept that: an output
+ * or monitoring thread that samples the field while other contexts on the
+ * same device keep stepping (cudaFree waits for the whole device, so the
+ * sample would stall every other simulation on it), and a process that has
+ * committed the device memory to lattices up to its budget, where a
+ * read-back must not fail for want of memory half-way through a run.  This
+ * variant builds the field in a fixed array of the library's own device image
+ * instead, so it needs no memory beyond what the library was loaded with.
+ *
+ * Limit: N_C <= D3Q19_STATIC_SPREAD_MAX_CELLS (3 floats a node, 3 MiB).
+ * The array exists once per device and process: calls that overlap in time on
+ * one device (two host threads, or two contexts on the same device) write the
+ * same array and race.  The first call on each device looks the array's
+ * address up (and with lazy module loading that makes the runtime load this
+ * file's device image); make that first call before any stream capture.
+ * ------------------------------------------------------------------------- */
+static __device__ __align__(256) float g_spread_static[3 * D3Q19_STATIC_SPREAD_MAX_CELLS];
+
+static constexpr int kStaticMaxDevices = 64;
+static std::mutex g_spread_static_mu;
+static float* g_spread_static_ptr[kStaticMaxDevices] = {nullptr};
+
+/* Once per device, with that device current: the device address of
+ * g_spread_static. */
+static int spread_static_address(d3q19_ctx* c, float** out) {
+  std::lock_guard<std::mutex> lock(g_spread_static_mu);
+  if (c->dev < 0 || c->dev >= kStaticMaxDevices)
+    return fail(c, D3Q19_EINVAL, "device %d: the static spread buffer is tracked for devices 0..%d only", c->dev,
+                kStaticMaxDevices - 1);
+  if (!g_spread_static_ptr[c->dev]) {
+    CUDA_TRY(c, cudaSetDevice(c->dev));
+    float* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_spread_static);
+    if (e != cudaSuccess || !ptr)
+      return fail(c, D3Q19_ECUDA, "cudaGetSymbolAddress(g_spread_static) on device %d: %s", c->dev,
+                  cudaGetErrorString(e));
+    g_spread_static_ptr[c->dev] = ptr;
+  }
+  *out = g_spread_static_ptr[c->dev];
+  return 0;
+}
+
+extern "C" int d3q19_read_spread_force_static(d3q19_ctx* c, float* gpf0) {
+  if (!c || !gpf0) return D3Q19_EINVAL;
+  const long long NC = c->g.NC;
+  if (NC > (long long)D3Q19_STATIC_SPREAD_MAX_CELLS)
+    return fail(c, D3Q19_EINVAL,
+                "lattice of %lld nodes exceeds the %d nodes of the static spread buffer; use d3q19_read_spread_force",
+                NC, (int)D3Q19_STATIC_SPREAD_MAX_CELLS);
+  float* field = nullptr;
+  int rc = spread_static_address(c, &field);
+  if (rc) return rc;
+  cudaSetDevice(c->dev);
+  /* Nodes no marker reaches read 0, and the spread kernels add into the
+   * field: the used part starts at zero on every call. */
+  CUDA_TRY(c, cudaMemsetAsync(field, 0, sizeof(float) * 3 * NC, c->stream));
+  if (c->ppar.np > 0) {
+    TileLists tl;
+    tl.cap = c->tile_cap;
+    tl.count = c->tile_count;
+    tl.list = c->tile_list;
+    tl.mrec = c->mrec;
+    tl.fmax = c->fmax;
+    if (c->opt.arithmetic == 1)
+      CUDA_TRY(c, launch_spread_field_exact(c->g, tl, c->ip.MaxSurfPointsPerNode, field, c->err, c->stream));
+    else
+      CUDA_TRY(c, launch_spread_field(c->g, tl, c->last_t, field, c->err, c->stream));
+  }
+  return readback(c, gpf0, (const float*)field, 3 * NC);
 }

@@ -16,6 +16,8 @@ LIBDIR = os.path.join(PKG, "lib")
 CUDA_LIB = os.path.join(LIBDIR, "libd3q19_b200.so")
 HOST_LIB = os.path.join(LIBDIR, "libd3q19_host.so")
 
+# Largest lattice (N_C nodes) d3q19_read_spread_force_static accepts.
+STATIC_SPREAD_MAX_CELLS = 262144
 STATUS = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ENODEV", -5: "EOVERFLOW", -6: "ENUMERIC",
           -7: "ESTATE"}
 
@@ -103,7 +105,8 @@ def cuda_lib():
         lib.d3q19_periodic_map.argtypes = [C.POINTER(IntParams), P, C.c_int]
         for name in ("d3q19_write_lattice", "d3q19_write_particles", "d3q19_write_zones", "d3q19_read_u",
                      "d3q19_read_tau", "d3q19_read_parkin", "d3q19_read_parforce", "d3q19_read_parfluidforce",
-                     "d3q19_read_f", "d3q19_read_spread_force", "d3q19_read_marker_cells", "d3q19_read_zones",
+                     "d3q19_read_f", "d3q19_read_spread_force", "d3q19_read_spread_force_static",
+                     "d3q19_read_marker_cells", "d3q19_read_zones",
                      "d3q19_synchronize", "d3q19_destroy", "d3q19_write_periodic_map"):
             getattr(lib, name).restype = C.c_int
         lib.d3q19_step.argtypes = [P, C.c_int]
@@ -322,6 +325,11 @@ class Simulation:
 
     def read_spread_force(self):
         return self._read("d3q19_read_spread_force", 3 * self.nc)
+
+    def read_spread_force_static(self):
+        """The spread force field through the entry point that allocates no
+        device memory (lattices of up to STATIC_SPREAD_MAX_CELLS nodes)."""
+        return self._read("d3q19_read_spread_force_static", 3 * self.nc)
 
     def read_marker_cells(self):
         return self._read("d3q19_read_marker_cells", 3 * self.np * self.ip.PointsPerParticle, np.int32)

@@ -204,6 +204,16 @@ int d3q19_read_f(d3q19_ctx* ctx, float* f);
 /* The spread IBM force field of the last step, as the reference's gpf slot 0
  * after sum_particle_fluid_forces (GPU_program.cl:258-289): float[3][N_C]. */
 int d3q19_read_spread_force(d3q19_ctx* ctx, float* gpf0);
+/* d3q19_read_spread_force without any device allocation (no counterpart in
+ * the reference): the field is built in a fixed array of the library's device
+ * image, for callers that may not allocate or free device memory while a run
+ * is under way.  Lattices of at most D3Q19_STATIC_SPREAD_MAX_CELLS nodes
+ * (N_C, buffer layers included); larger ones return D3Q19_EINVAL.  One array
+ * per device and process: calls that overlap in time on the same device race.
+ * The first call on each device does a one-time set-up (looks the array up);
+ * make it before any stream capture. */
+#define D3Q19_STATIC_SPREAD_MAX_CELLS 262144
+int d3q19_read_spread_force_static(d3q19_ctx* ctx, float* gpf0);
 /* Corner cell (x_i0, y_i0, z_i0) of every marker of the last step
  * (GPU_program.cl:150-156): int[3*TotalSurfPoints]. */
 int d3q19_read_marker_cells(d3q19_ctx* ctx, int* cells);
