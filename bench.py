@@ -29,7 +29,10 @@ PKG = os.path.join(REPO, "dispersion-shear_d3q19-opencl_b200")
 sys.path.insert(0, PKG)
 sys.path.insert(0, REPO)
 
-BYTES_PER_NODE = 152  # 19 populations read + 19 written, FP32
+# Algorithmic bytes per lattice node and step: 19 populations read + 19
+# written, FP32 (4 B) or 16-bit shifted storage (2 B).
+STORAGE = {"fp32": (0, 152, "f32"), "fp16": (1, 76, "f32 arithmetic, f16 shifted storage"),
+           "bf16": (2, 76, "f32 arithmetic, bf16 shifted storage")}
 
 WORKLOADS = {
     "dense-powerlaw-128": dict(
@@ -41,9 +44,24 @@ WORKLOADS = {
         z_wall_particle_buffer=9.0, domain_decomposition=(1, 1, 1), rebuild_neigh_list_freq=10,
         particle_collision_params=2.0, video_freq=1000000, shear_stress_freq=1000000, console_print_freq=1000000),
 }
+# The same fluid without spheres (fluid kernel alone; a profiling aid).
+WORKLOADS["powerlaw-128-fluid"] = dict(WORKLOADS["dense-powerlaw-128"], num_particles=0)
+# 64^3 Couette flow past one fixed sphere of diameter 16 with 256 markers at
+# the box centre, Newtonian tau = 0.8, walls +-0.02 (the reference's own
+# CPU-runnable single-sphere case).
+WORKLOADS["couette-sphere-64"] = dict(
+    iterations=2000, total_lattice_size=(64, 64, 64), boundary_conditions_xyz=(0, 0, 1), newtonian_tau=0.8,
+    viscosity_model=1, velocity_bc_upper=(0.02, 0.0, 0.0), velocity_bc_lower=(-0.02, 0.0, 0.0), initial_f="constant",
+    initial_vel=(0.0, 0.0, 0.0), num_particles=1, particle_diameter=16.0, ibm_points_per_particle=256,
+    fixed_particles=1, initial_particle_distribution=3, initial_particle_buffer=31.0, z_wall_particle_buffer=2.0,
+    domain_decomposition=(1, 1, 1), rebuild_neigh_list_freq=10, video_freq=1000000, shear_stress_freq=1000000,
+    console_print_freq=1000000)
 DESCRIPTION = {
     "dense-powerlaw-128": "dense power-law suspension: 128^3 lattice, 200 spheres d=16 (512 markers, RSA seed 1, "
                           "gap 2), n=0.6 k=0.0105 tau in [0.55,2], walls +-0.05",
+    "powerlaw-128-fluid": "power-law fluid alone: 128^3 lattice, n=0.6 k=0.0105 tau in [0.55,2], walls +-0.05",
+    "couette-sphere-64": "Couette flow past one fixed sphere: 64^3 lattice, Newtonian tau 0.8, walls +-0.02, "
+                         "d=16 with 256 markers at the centre",
 }
 
 # The same workload as the reference host can express it: its marker rule
@@ -58,6 +76,25 @@ REFERENCE_KEYWORDS = {
         initial_particle_buffer=8.0, z_wall_particle_buffer=2.0, domain_decomposition=(1, 1, 1),
         rebuild_neigh_list_freq=10, particle_collision_params=2.0, video_freq=1000000, shear_stress_freq=1000000,
         console_print_freq=1000000),
+}
+
+
+REFERENCE_KEYWORDS["powerlaw-128-fluid"] = dict(REFERENCE_KEYWORDS["dense-powerlaw-128"], num_particles=0)
+# The reference has no fixed spheres and derives 1024 markers for d = 16.
+REFERENCE_KEYWORDS["couette-sphere-64"] = dict(
+    total_lattice_size=(64, 64, 64), boundary_conditions_xyz=(0, 0, 1), newtonian_tau=0.8, viscosity_model=1,
+    velocity_bc_upper=(0.02, 0.0, 0.0), velocity_bc_lower=(-0.02, 0.0, 0.0), initial_f="constant",
+    initial_vel=(0.0, 0.0, 0.0), num_particles=1, particle_diameter=16.0, initial_particle_distribution=3,
+    initial_particle_buffer=31.0, z_wall_particle_buffer=2.0, domain_decomposition=(1, 1, 1),
+    rebuild_neigh_list_freq=10, video_freq=1000000, shear_stress_freq=1000000, console_print_freq=1000000)
+# Which reference build runs the workload (with or without USE_CONSTANT_VISCOSITY).
+REFERENCE_VARIABLE = {"dense-powerlaw-128": True, "powerlaw-128-fluid": True, "couette-sphere-64": False}
+REFERENCE_NOTE = {
+    "dense-powerlaw-128": "the 128^3 lattice with 200 d=16 spheres; reference marker rule (1024/sphere) and "
+                          "jittered-grid placement",
+    "powerlaw-128-fluid": "the 128^3 power-law lattice without spheres",
+    "couette-sphere-64": "the 64^3 Couette lattice with one d=16 sphere (reference marker rule: 1024 markers; "
+                         "the reference integrates the sphere)",
 }
 
 
@@ -136,10 +173,11 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(workload):
+def ncu_traffic(workload, storage="fp32"):
     """DRAM bytes per launch of the collide-stream kernel from the committed
     ncu summary (profiles/), or None."""
-    p = os.path.join(REPO, "profiles", f"fluid_step_kernel_{workload}.json")
+    suffix = "" if storage == "fp32" else "_" + storage
+    p = os.path.join(REPO, "profiles", f"fluid_step_kernel_{workload}{suffix}.json")
     try:
         with open(p) as fh:
             d = json.load(fh)
@@ -148,7 +186,7 @@ def ncu_traffic(workload):
         return None
 
 
-def setup(workload, device):
+def setup(workload, device, storage="fp32"):
     import numpy as np  # noqa: F401
 
     import d3q19_b200 as d3
@@ -156,16 +194,20 @@ def setup(workload, device):
     cfg = d3.parse_config(d3.keywords_text(WORKLOADS[workload]))
     hs = d3.HostState(cfg, data_dir=os.getcwd())
     hs.options.device = device
-    sim = d3.Simulation.from_host_state(hs, device=device)
+    hs.options.storage = STORAGE[storage][0]
+    sim = d3.Simulation.from_host_state(hs, device=device, storage=STORAGE[storage][0])
     return d3, hs, sim
 
 
 def launches(ip, rebuild, t0, k):
+    """Kernels one step sequence launches: the fluid step, and with spheres
+    the particle pass, the contact forces and (every rebuild steps) the zone
+    rebuild."""
     n = 0
     for t in range(t0, t0 + k):
         n += 1
         if ip.NumParticles > 0:
-            n += 1 + (1 if t % rebuild == 0 else 0)
+            n += 2 + (1 if t % rebuild == 0 else 0)
     return n
 
 
@@ -174,7 +216,8 @@ def run_ours(args, rank, world, local_rank, dist):
     import torch
 
     torch.cuda.set_device(local_rank)
-    d3, hs, sim = setup(args.workload, local_rank)
+    d3, hs, sim = setup(args.workload, local_rank, args.storage)
+    bytes_per_node = STORAGE[args.storage][1]
     ip = hs.cfg.ip
     interior = (ip.LatticeSize[0] - 2) * (ip.LatticeSize[1] - 2) * (ip.LatticeSize[2] - 2)
     R = hs.cfg.hp.RebuildFreq
@@ -260,24 +303,25 @@ def run_ours(args, rank, world, local_rank, dist):
     if rank != 0:
         return None
     peak, peak_kind = measured_peak()
-    achieved = BYTES_PER_NODE * interior / (fluid_avg * 1e-3) / 1e9
+    achieved = bytes_per_node * interior / (fluid_avg * 1e-3) / 1e9
     value = world * interior * args.steps / (ms_max * 1e-3) / 1e6
     out = {
         "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded RSA placement)",
+        "scaling": "weak", "vs_baseline": None, "dtype": STORAGE[args.storage][2],
+        "data": "synthetic (seeded RSA placement)",
         "impl": "ours",
         "config": {"workload": args.workload, "description": DESCRIPTION[args.workload],
                    "lattice": list(ip.LatticeSize), "interior_nodes": interior, "spheres": ip.NumParticles,
                    "markers_per_sphere": ip.PointsPerParticle, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (2 x 19 x 4 B x 2.1 M nodes = 320 MB distributions)"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": ncu_traffic(args.workload),
-                     "kernel": "fluid_step_kernel", "bytes_per_node": BYTES_PER_NODE,
+                     "frac": round(achieved / peak, 4), "traffic": ncu_traffic(args.workload, args.storage),
+                     "kernel": "fluid_step_kernel", "bytes_per_node": bytes_per_node,
                      "kernel_ms": round(fluid_avg, 5), "particle_kernel_ms": round(part_avg, 5),
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                      "fallback 6.65 TB/s",
-                     "step_frac": round(value / world * 1e6 * BYTES_PER_NODE / 1e9 / peak, 4)},
+                     "step_frac": round(value / world * 1e6 * bytes_per_node / 1e9 / peak, 4)},
         "e2e": {"value": round(world * interior * args.steps / e2e_s / 1e6, 1), "unit": "MLUPS",
                 "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                 "note": "C-ABI calls from pinned host buffers: upload of the initial state, K steps, read-back "
@@ -298,7 +342,7 @@ def _reference_run(workload, iters, threads):
 
     kw = dict(REFERENCE_KEYWORDS[workload], iterations=iters)
     t0 = time.perf_counter()
-    po.run_reference(kw, variable_viscosity=True, serial=False, dump=False, threads=threads,
+    po.run_reference(kw, variable_viscosity=REFERENCE_VARIABLE[workload], serial=False, dump=False, threads=threads,
                      workdir=tempfile.mkdtemp(prefix="d3q19bench_"))
     return time.perf_counter() - t0
 
@@ -317,11 +361,11 @@ def cpu_baseline(workload, sample_steps=8):
         tb = _reference_run(workload, 1 + sample_steps, threads)
         per = max(tb - ta, 1e-9) / sample_steps
         return {"value": round(interior / per / 1e6, 3), "unit": "MLUPS", "cores": threads, "kind": "reference",
-                "sample": f"{sample_steps} steps of the reference's own program (GPU_program.cl without "
-                          "USE_CONSTANT_VISCOSITY + CPU_program.cl + D3Q19-OpenCL.c, mock OpenCL runtime, "
-                          f"{threads} OpenMP threads) on the 128^3 lattice with 200 d=16 spheres; per-step time from "
-                          "the difference of a 1-step and a 9-step run; reference marker rule (1024/sphere) and "
-                          "jittered-grid placement"}
+                "sample": f"{sample_steps} steps of the reference's own program (GPU_program.cl "
+                          f"{'without' if REFERENCE_VARIABLE[workload] else 'with'} USE_CONSTANT_VISCOSITY + "
+                          "CPU_program.cl + D3Q19-OpenCL.c, mock OpenCL runtime, "
+                          f"{threads} OpenMP threads) on {REFERENCE_NOTE[workload]}; per-step time from the "
+                          f"difference of a 1-step and a {1 + sample_steps}-step run"}
     return {"value": None, "unit": "MLUPS", "cores": threads, "kind": "reference",
             "sample": "oracle/_ref not built on this machine"}
 
@@ -351,6 +395,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dense-powerlaw-128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--storage", default="fp32", choices=sorted(STORAGE),
+                    help="distribution storage: fp32 (the reference's), or 16-bit shifted")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

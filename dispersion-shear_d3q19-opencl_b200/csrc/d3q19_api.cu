@@ -29,7 +29,7 @@ struct d3q19_ctx {
   Geom g;
   FluidParams fpar;
   ParticleParams ppar;
-  float* f[2] = {nullptr, nullptr};
+  void* f[2] = {nullptr, nullptr};  // float, or 16-bit shifted storage (opt.storage)
   int cur = 0;         // f[cur] is what the next step reads
   int f_state = 0;     // 0 unset, 1 reference state (pre-collision), 2 post-collision
   float* u = nullptr;
@@ -67,6 +67,8 @@ struct d3q19_ctx {
 };
 
 static char g_create_error[512] = {0};
+
+static int ensure_scratch(d3q19_ctx* c, size_t bytes);
 
 static int fail(d3q19_ctx* c, int code, const char* fmt, ...) {
   char* buf = c ? c->msg : g_create_error;
@@ -112,6 +114,8 @@ extern "C" int d3q19_get_device_info(int device, d3q19_device_info* out) {
 }
 
 static int validate(const int_param_struct* ip, const flp_param_struct* fp, const d3q19_options* o) {
+  if ((long long)ip->LatticeSize[0] * ip->LatticeSize[1] * ip->LatticeSize[2] >= (1LL << 31))
+    return fail(nullptr, D3Q19_EINVAL, "lattice of 2^31 or more nodes");
   for (int d = 0; d < 3; d++) {
     if (ip->LatticeSize[d] < 4 || ip->LatticeSize[d] > 65535)
       return fail(nullptr, D3Q19_EINVAL, "LatticeSize[%d] = %d outside [4, 65535]", d, ip->LatticeSize[d]);
@@ -131,7 +135,10 @@ static int validate(const int_param_struct* ip, const flp_param_struct* fp, cons
     return fail(nullptr, D3Q19_EINVAL, "the reference-exact arithmetic has the reference's tau limits only");
   if (o->arithmetic == 1 && (ip->MaxSurfPointsPerNode < 1 || ip->MaxSurfPointsPerNode > 16))
     return fail(nullptr, D3Q19_EINVAL, "MaxSurfPointsPerNode must be in [1, 16] for the reference-exact arithmetic");
-  if (o->storage != 0) return fail(nullptr, D3Q19_EINVAL, "storage %d not available in this build", o->storage);
+  if (o->storage < 0 || o->storage > 2)
+    return fail(nullptr, D3Q19_EINVAL, "storage %d (0 FP32, 1 FP16 shifted, 2 BF16 shifted)", o->storage);
+  if (o->arithmetic == 1 && o->storage != 0)
+    return fail(nullptr, D3Q19_EINVAL, "the reference-exact arithmetic stores FP32 distributions only");
   if (o->particle_precision != 0)
     return fail(nullptr, D3Q19_EINVAL, "particle_precision %d not available in this build", o->particle_precision);
   if (fp->NewtonianTau <= 0.5f) return fail(nullptr, D3Q19_EINVAL, "NewtonianTau must exceed 0.5");
@@ -240,7 +247,9 @@ extern "C" int d3q19_create(const int_param_struct* ip, const flp_param_struct* 
   pp.exact = o.arithmetic == 1 ? 1 : 0;
 
   const long long NC = g.NC;
-  if ((rc = dalloc(c, &c->f[0], 19 * NC)) || (rc = dalloc(c, &c->f[1], 19 * NC)) || (rc = dalloc(c, &c->u, 3 * NC)) ||
+  const size_t fbytes = (size_t)storage_bytes(o.storage) * 19 * NC;
+  if ((rc = dalloc(c, (char**)&c->f[0], fbytes)) || (rc = dalloc(c, (char**)&c->f[1], fbytes)) ||
+      (rc = dalloc(c, &c->u, 3 * NC)) ||
       (rc = dalloc(c, &c->tau, NC)) || (rc = dalloc(c, &c->err, 1)) || (rc = dalloc(c, &c->clamps, 1))) {
     snprintf(g_create_error, sizeof(g_create_error), "%s", c->msg);
     d3q19_destroy(c);
@@ -294,7 +303,16 @@ extern "C" int d3q19_write_lattice(d3q19_ctx* c, const float* f, const float* u,
   if (!c || !f || !u) return D3Q19_EINVAL;
   cudaSetDevice(c->dev);
   const long long NC = c->g.NC;
-  CUDA_TRY(c, cudaMemcpyAsync(c->f[c->cur], f, sizeof(float) * 19 * NC, cudaMemcpyHostToDevice, c->stream));
+  if (c->opt.storage == STORE_F32) {
+    CUDA_TRY(c, cudaMemcpyAsync(c->f[c->cur], f, sizeof(float) * 19 * NC, cudaMemcpyHostToDevice, c->stream));
+  } else {
+    // Upload in FP32, then round to the shifted 16-bit form on the device.
+    int rc = ensure_scratch(c, sizeof(float) * 19 * NC);
+    if (rc) return rc;
+    CUDA_TRY(c, cudaMemcpyAsync(c->scratch, f, sizeof(float) * 19 * NC, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, launch_store_f((const float*)c->scratch, c->f[c->cur], NC, c->opt.storage, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
   CUDA_TRY(c, cudaMemcpyAsync(c->u, u, sizeof(float) * 3 * NC, cudaMemcpyHostToDevice, c->stream));
   if (tau_lb) {
     CUDA_TRY(c, cudaMemcpyAsync(c->tau, tau_lb, sizeof(float) * NC, cudaMemcpyHostToDevice, c->stream));
@@ -484,7 +502,8 @@ static int enqueue_step(d3q19_ctx* c, int t) {
     CUDA_TRY(c, launch_fluid_exact(fa, c->f_state == 1, c->opt.variable_viscosity != 0, c->ip.MaxSurfPointsPerNode,
                                    c->stream));
   else
-    CUDA_TRY(c, launch_fluid(fa, c->f_state == 1, c->opt.variable_viscosity != 0, c->opt.collision, c->stream));
+    CUDA_TRY(c, launch_fluid(fa, c->f_state == 1, c->opt.variable_viscosity != 0, c->opt.collision, c->opt.storage,
+                             c->stream));
   if (c->profiling) {
     CUDA_TRY(c, cudaEventRecord(e1, c->stream));
     c->ev_fluid.emplace_back(e0, e1);
@@ -657,16 +676,20 @@ extern "C" int d3q19_read_f(d3q19_ctx* c, float* f) {
   if (c->f_state == 0) return fail(c, D3Q19_ESTATE, "lattice not written");
   cudaSetDevice(c->dev);
   const long long NC = c->g.NC;
-  if (c->f_state == 1) return readback(c, f, (const float*)c->f[c->cur], 19 * NC);
+  if (c->f_state == 1 && c->opt.storage == STORE_F32) return readback(c, f, (const float*)c->f[c->cur], 19 * NC);
   int rc = ensure_scratch(c, sizeof(float) * 19 * NC);
   if (rc) return rc;
+  if (c->f_state == 1) {
+    CUDA_TRY(c, launch_load_f(c->f[c->cur], (float*)c->scratch, NC, c->opt.storage, c->stream));
+    return readback(c, f, (const float*)c->scratch, 19 * NC);
+  }
   FluidArgs fa;
   memset(&fa, 0, sizeof(fa));
   fa.g = c->g;
   fa.p = c->fpar;
   fa.fin = c->f[c->cur];
   CUDA_TRY(c, cudaMemsetAsync(c->scratch, 0, sizeof(float) * 19 * NC, c->stream));
-  CUDA_TRY(c, launch_materialize_f(fa, (float*)c->scratch, c->stream));
+  CUDA_TRY(c, launch_materialize_f(fa, c->opt.storage, (float*)c->scratch, c->stream));
   return readback(c, f, (const float*)c->scratch, 19 * NC);
 }
 

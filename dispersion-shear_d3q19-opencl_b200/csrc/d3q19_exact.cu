@@ -434,7 +434,7 @@ __global__ void __launch_bounds__(FLUID_THREADS) fluid_exact_kernel(const FluidA
     float f[19];
     if (FIRST) {
 #pragma unroll
-      for (int q = 0; q < 19; q++) f[q] = a.fin[q * NC + i];
+      for (int q = 0; q < 19; q++) f[q] = ((const float*)a.fin)[q * NC + i];
     } else {
       const int Nxy = g.Nx * g.Ny;
       const int dxm = (g.periodic[0] && x == 1) ? g.Nx - 3 : -1;
@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(FLUID_THREADS) fluid_exact_kernel(const FluidA
         const int cx = CXQ(q), cy = CYQ(q), cz = CZQ(q);
         const long long src = i + (cx == 1 ? dxm : (cx == -1 ? dxp : 0)) + (cy == 1 ? dym : (cy == -1 ? dyp : 0)) +
                               (cz == 1 ? dzm : (cz == -1 ? dzp : 0));
-        f[q] = a.fin[q * NC + src];
+        f[q] = ((const float*)a.fin)[q * NC + src];
       }
       if (g.wallAxis >= 0) {
         const int c[3] = {x, y, z}, N[3] = {g.Nx, g.Ny, g.Nz};
@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(FLUID_THREADS) fluid_exact_kernel(const FluidA
       nclamp += clamped ? 1 : 0;
     }
 #pragma unroll
-    for (int q = 0; q < 19; q++) a.fout[q * NC + i] = f[q];
+    for (int q = 0; q < 19; q++) ((float*)a.fout)[q * NC + i] = f[q];
   }
   if (VAR && nclamp) atomicAdd(a.clamps, (unsigned long long)nclamp);
 }

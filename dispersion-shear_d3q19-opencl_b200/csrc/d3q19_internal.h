@@ -70,8 +70,10 @@ struct FluidArgs {
   Geom g;
   FluidParams p;
   int t;  // time step (selects the marker-force maximum slot)
-  const float* fin;
-  float* fout;
+  // Distributions, 19 rows of N_C values (q-major): float, or with 16-bit
+  // storage the shifted value f_q - w_q as IEEE half or bfloat16 bits.
+  const void* fin;
+  void* fout;
   float* u;
   float* tau;
   TileLists tiles;
@@ -132,8 +134,16 @@ struct ZoneArgs {
 };
 
 // Launchers (d3q19_kernels.cu).
-cudaError_t launch_fluid(const FluidArgs& a, bool first, bool variable, int collision, cudaStream_t s);
-cudaError_t launch_materialize_f(const FluidArgs& a, float* out, cudaStream_t s);
+// Storage of the distributions: 0 float, 1 half (f - w), 2 bfloat16 (f - w).
+constexpr int STORE_F32 = 0, STORE_F16 = 1, STORE_BF16 = 2;
+inline int storage_bytes(int storage) { return storage == STORE_F32 ? 4 : 2; }
+
+cudaError_t launch_fluid(const FluidArgs& a, bool first, bool variable, int collision, int storage, cudaStream_t s);
+cudaError_t launch_materialize_f(const FluidArgs& a, int storage, float* out, cudaStream_t s);
+// Conversions between float distributions and the stored form (n values,
+// row q of each N_C-long row block shifted by w_q).
+cudaError_t launch_store_f(const float* in, void* out, long long NC, int storage, cudaStream_t s);
+cudaError_t launch_load_f(const void* in, float* out, long long NC, int storage, cudaStream_t s);
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s);
 cudaError_t launch_zones(const ZoneArgs& a, cudaStream_t s);
 cudaError_t launch_spread_field(const Geom& g, const TileLists& t, int last_step, float* out, unsigned* err,

@@ -31,6 +31,8 @@
 //   update_particle_zones (CPU_program.cl:280-315) -> zone_rebuild_kernel.
 #include "d3q19_internal.h"
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -51,6 +53,38 @@ namespace d3q19 {
                  (q) == 7 ? 12 : (q) == 12 ? 7 : (q) == 8 ? 11 : (q) == 11 ? 8 : \
                  (q) == 9 ? 14 : (q) == 14 ? 9 : (q) == 10 ? 13 : (q) == 13 ? 10 : \
                  (q) == 15 ? 18 : (q) == 18 ? 15 : (q) == 16 ? 17 : 16)
+
+// ---------------------------------------------------------------------------
+// Distribution storage.  ST = float keeps f_q itself; the 16-bit forms keep
+// the shifted value f_q - w_q (w_q the rest-state weight 1/3, 1/18, 1/36),
+// whose magnitude is a small fraction of w_q, so the 16-bit significand
+// spends its bits on the deviation from rest.  Arithmetic stays FP32; the
+// stored value is rounded to nearest even once per step.
+#define WQ(q) ((q) == 0 ? (1.0f / 3.0f) : (q) <= 6 ? (1.0f / 18.0f) : (1.0f / 36.0f))
+
+template <typename ST>
+struct Stored;
+template <>
+struct Stored<float> {
+  static __device__ __forceinline__ float load(const float* p, float) { return __ldg(p); }
+  static __device__ __forceinline__ void store(float* p, float v, float) { *p = v; }
+};
+template <>
+struct Stored<__half> {
+  static __device__ __forceinline__ float load(const __half* p, float w) {
+    return __half2float(__ushort_as_half(__ldg(reinterpret_cast<const unsigned short*>(p)))) + w;
+  }
+  static __device__ __forceinline__ void store(__half* p, float v, float w) { *p = __float2half_rn(v - w); }
+};
+template <>
+struct Stored<__nv_bfloat16> {
+  static __device__ __forceinline__ float load(const __nv_bfloat16* p, float w) {
+    return __bfloat162float(__ushort_as_bfloat16(__ldg(reinterpret_cast<const unsigned short*>(p)))) + w;
+  }
+  static __device__ __forceinline__ void store(__nv_bfloat16* p, float v, float w) {
+    *p = __float2bfloat16_rn(v - w);
+  }
+};
 
 // ---------------------------------------------------------------------------
 // Wet-node velocity boundary (GPU_program.cl:737-865 with calcRho = 0, the
@@ -99,32 +133,35 @@ __device__ __forceinline__ void apply_wall(float (&f)[19], int axis, int side, c
   }
 }
 
-// Local relaxation time (GPU_program.cl:1041-1128).  Optional extensions:
-// an upper clamp and a regularised Casson yield term.
+// Local relaxation time (GPU_program.cl:1041-1128), with the hardware
+// approximations of the reciprocal, reciprocal square root and power
+// (a few ulp; the reference-exact arithmetic evaluates them as written).
+// Optional extensions: an upper clamp and a regularised Casson yield term.
 __device__ __forceinline__ float compute_tau(const FluidParams& p, float srt, bool& clamped) {
   float tau = p.tauN;
   const float eps = 1e-8f;
   if (p.viscModel == 2) {  // power law
     float k = p.visc[0], n = p.visc[1], nu;
     srt = srt > eps ? srt : eps;
-    if (n == 0.5f) nu = k / sqrtf(srt);
+    if (n == 0.5f) nu = k * rsqrtf(srt);
     else if (n == 1.0f) nu = k;
     else if (n == 2.0f) nu = k * srt;
-    else nu = k * powf(srt, n - 1.0f);
+    else nu = k * exp2f(__log2f(srt) * (n - 1.0f));
     tau = 3.0f * nu + 0.5f;
   } else if (p.viscModel == 4) {  // Casson
     float tY = p.visc[0], eta = p.visc[1];
     srt = srt > eps ? srt : eps;
-    float sr = p.cassonReg > 0.0f ? sqrtf(srt * srt + p.cassonReg * p.cassonReg) : srt;
-    float a = sqrtf(tY / sr) + sqrtf(eta);
+    float sr2 = p.cassonReg > 0.0f ? srt * srt + p.cassonReg * p.cassonReg : srt * srt;
+    float a = sqrtf(tY * rsqrtf(sr2)) + sqrtf(eta);
     tau = 3.0f * (a * a) + 0.5f;
   } else if (p.viscModel == 3) {  // Herschel-Bulkley
     float tY = p.visc[0], k = p.visc[1], n = p.visc[2], nu;
     srt = srt > eps ? srt : eps;
-    if (n == 0.5f) nu = tY / srt + k / sqrtf(srt);
-    else if (n == 1.0f) nu = tY / srt + k;
-    else if (n == 2.0f) nu = tY / srt + k * srt;
-    else nu = tY / srt + k * powf(srt, n - 1.0f);
+    const float yield = __fdividef(tY, srt);
+    if (n == 0.5f) nu = yield + k * rsqrtf(srt);
+    else if (n == 1.0f) nu = yield + k;
+    else if (n == 2.0f) nu = yield + k * srt;
+    else nu = yield + k * exp2f(__log2f(srt) * (n - 1.0f));
     tau = 3.0f * nu + 0.5f;
   } else {
     return tau;
@@ -135,7 +172,10 @@ __device__ __forceinline__ float compute_tau(const FluidParams& p, float srt, bo
       tau = p.tauMin;
       clamped = true;
     }
-  } else if ((double)tau < 0.505) {  // MIN_TAU is a double constant (GPU_program.cl:6)
+  } else if (tau <= 0.505f) {
+    // The reference compares with the double constant MIN_TAU = 0.505
+    // (GPU_program.cl:6); (double)tau < 0.505 holds exactly for the floats
+    // up to and including 0.505f, which lies below 0.505.
     tau = 0.505f;
     clamped = true;
   }
@@ -147,14 +187,18 @@ __device__ __forceinline__ float compute_tau(const FluidParams& p, float srt, bo
 // population q of node i comes from node i - c_q, wrapped on periodic axes.
 // On a wall plane the sources outside the lattice interior are the buffer
 // layer; those populations are unknowns and are rebuilt by velocity_bc.
-__device__ __forceinline__ void gather(float (&f)[19], const float* __restrict__ fin, long long NC, long long i,
-                                       int dxm, int dxp, int dym, int dyp, int dzm, int dzp) {
+// Addressing: row q of the distributions starts at fin + q*NC (a 64-bit
+// offset, the same for every thread); within a row the node index is a
+// 32-bit int (N_C < 2^31 is checked when the context is created).
+template <typename ST>
+__device__ __forceinline__ void gather(float (&f)[19], const ST* __restrict__ fin, long long NC, int i, int dxm,
+                                       int dxp, int dym, int dyp, int dzm, int dzp) {
 #pragma unroll
   for (int q = 0; q < 19; q++) {
     const int cx = CXQ(q), cy = CYQ(q), cz = CZQ(q);
-    long long src = i + (cx == 1 ? dxm : (cx == -1 ? dxp : 0)) + (cy == 1 ? dym : (cy == -1 ? dyp : 0)) +
+    const int src = i + (cx == 1 ? dxm : (cx == -1 ? dxp : 0)) + (cy == 1 ? dym : (cy == -1 ? dyp : 0)) +
                     (cz == 1 ? dzm : (cz == -1 ? dzp : 0));
-    f[q] = __ldg(fin + q * NC + src);
+    f[q] = Stored<ST>::load(fin + q * NC + src, WQ(q));
   }
 }
 
@@ -212,12 +256,16 @@ __device__ __forceinline__ void boundaries(float (&f)[19], const Geom& g, const 
 // vector with 1/tau at rows 8,9,10,14,15 (GPU_program.cl:453, 567-568);
 // COLL 1: BGK.
 template <int COLL, bool VAR>
-__device__ __forceinline__ void collide(float (&f)[19], float rho, float ux, float uy, float uz, float gx, float gy,
-                                        float gz, float& tau, const FluidParams& p, bool& clamped) {
+__device__ __forceinline__ void collide(float (&f)[19], float rho, float ir, float ux, float uy, float uz, float gx,
+                                        float gy, float gz, float& tau, const FluidParams& p, bool& clamped) {
   // Equilibrium minus f, pairwise (GPU_program.cl:978-1007), and the Guo term
   // (GPU_program.cl:1010-1038): for a pair +-c the even parts are shared.
   const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
   const float uDg = ux * gx + uy * gy + uz * gz;
+  // Correctly rounded rho/3, rho/18, rho/36 as the reference's equilibrium
+  // (GPU_program.cl:978-1007): a fluid at rest then has exactly zero
+  // non-equilibrium part, which the strain rate of a power-law or yield-
+  // stress fluid at rest depends on.
   const float r0 = rho / 3.0f, r1 = rho / 18.0f, r2 = rho / 36.0f;
   float d[19], base[19];
   {
@@ -295,7 +343,7 @@ __device__ __forceinline__ void collide(float (&f)[19], float rho, float ux, flo
     // Strain rate from the relaxed non-equilibrium moments with tau(t-1)
     // (GPU_program.cl:459-562): the second moments of M^-1 S_old M d, which
     // only rows e, 3pxx, pww and the off-diagonal p carry.
-    const float it = 1.0f / tau;
+    const float it = __fdividef(1.0f, tau);
     float a1, a9, a11, a13, a14, a15;
     if (COLL == 0) {
       a1 = s1 * m1 * INV_N1; a9 = it * m9 * INV_N9; a11 = s11 * m11 * INV_N11;
@@ -309,11 +357,11 @@ __device__ __forceinline__ void collide(float (&f)[19], float rho, float ux, flo
     const float szz = 42.0f * a1 - 6.0f * a9 - 6.0f * a11;
     const float sxy = 4.0f * a13, syz = 4.0f * a14, sxz = 4.0f * a15;
     const float ss = sxx * sxx + 2.0f * (sxy * sxy + sxz * sxz + syz * syz) + syy * syy + szz * szz;
-    const float srt = sqrtf(ss) * 2.1213203f / rho;
+    const float srt = sqrtf(ss) * 2.1213203f * ir;
     tau = compute_tau(p, srt, clamped);
   }
 
-  const float it = 1.0f / tau;
+  const float it = __fdividef(1.0f, tau);
   float a1, a2, a3, a4, a5, a6, a7, a8, a9, a10, a11, a12, a13, a14, a15, a16, a17, a18;
   if (COLL == 0) {
     a3 = 0.1f * m3; a5 = 0.1f * m5; a7 = 0.1f * m7;
@@ -367,7 +415,7 @@ __device__ __forceinline__ void collide(float (&f)[19], float rho, float ux, flo
 // Spread force of one tile: accumulate -w*F of every listed marker on the
 // tile plus a one-node halo (the reference's gpf slot sum, GPU_program.cl:
 // 210-227 and 258-289) in 2^-40 fixed point, then convert to float.
-struct SpreadSmem {
+struct __align__(16) SpreadSmem {
   int hi[3][HALO_N];        // sum of the high parts (v >> 16)
   unsigned lo[3][HALO_N];   // sum of the low 16 bits
   float g[3][HALO_N];       // the spread force of the halo nodes
@@ -409,9 +457,10 @@ __device__ __forceinline__ int fixed_exponent(unsigned fmax_bits) {
 // parts; the sum is converted back once.
 __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& tl, long long T, int n, int X0,
                                 int Y0, int Z0, int tid, int nthreads, int k, unsigned* err) {
-  for (int h = tid; h < 3 * HALO_N; h += nthreads) {
-    (&s.hi[0][0])[h] = 0;
-    (&s.lo[0][0])[h] = 0u;
+  static_assert((3 * HALO_N) % 4 == 0, "halo arrays are cleared and converted four words at a time");
+  {
+    int4* z4 = reinterpret_cast<int4*>(&s.hi[0][0]);  // hi and lo are contiguous
+    for (int h = tid; h < 2 * 3 * HALO_N / 4; h += nthreads) z4[h] = make_int4(0, 0, 0, 0);
   }
   __syncthreads();
   const float scale = ldexpf(1.0f, k);
@@ -447,17 +496,28 @@ __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& t
     }
   }
   __syncthreads();
-  const float inv = ldexpf(1.0f, -k);
-  for (int h = tid; h < 3 * HALO_N; h += nthreads) {
-    const long long v = (long long)(&s.hi[0][0])[h] * 65536LL + (long long)(&s.lo[0][0])[h];
-    (&s.g[0][0])[h] = __ll2float_rn(v) * inv;
+  // value = (hi * 2^16 + lo) * 2^-k, both parts scaled exactly by powers of
+  // two and joined with one rounding.
+  const float inv = ldexpf(1.0f, -k), inv_hi = ldexpf(1.0f, 16 - k);
+  {
+    const int4* h4 = reinterpret_cast<const int4*>(&s.hi[0][0]);
+    const uint4* l4 = reinterpret_cast<const uint4*>(&s.lo[0][0]);
+    float4* g4 = reinterpret_cast<float4*>(&s.g[0][0]);
+    for (int h = tid; h < 3 * HALO_N / 4; h += nthreads) {
+      const int4 a = h4[h];
+      const uint4 b = l4[h];
+      g4[h] = make_float4(__fmaf_rn((float)a.x, inv_hi, (float)b.x * inv), __fmaf_rn((float)a.y, inv_hi, (float)b.y * inv),
+                          __fmaf_rn((float)a.z, inv_hi, (float)b.z * inv), __fmaf_rn((float)a.w, inv_hi, (float)b.w * inv));
+    }
   }
   __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
-template <bool FIRST, bool VAR, int COLL>
+template <bool FIRST, bool VAR, int COLL, typename ST>
 __global__ void __launch_bounds__(FLUID_THREADS, 4) fluid_step_kernel(const FluidArgs a) {
+  const ST* __restrict__ fin = static_cast<const ST*>(a.fin);
+  ST* __restrict__ fout = static_cast<ST*>(a.fout);
   __shared__ SpreadSmem sm;
   __shared__ int s_cnt;
   const Geom& g = a.g;
@@ -486,65 +546,84 @@ __global__ void __launch_bounds__(FLUID_THREADS, 4) fluid_step_kernel(const Flui
   const int x = X0 + threadIdx.x;
   const int y = Y0 + threadIdx.y;
   const long long NC = g.NC;
-  const float sten[3] = {0.25f, 0.5f, 0.25f};
+  // Each thread takes two consecutive z-planes, so the 27-point smoothing
+  // (weights 1/4, 1/2, 1/4 per axis) shares the 9-point x-y sums of the two
+  // middle halo planes between its nodes.
+  float sg[2][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+  if (cnt > 0) {
+    const int hx = threadIdx.x + 1, hy = threadIdx.y + 1, hz0 = 2 * threadIdx.z;
+#pragma unroll
+    for (int pl = 0; pl < 4; pl++) {
+      float px = 0.0f, py = 0.0f, pz = 0.0f;
+#pragma unroll
+      for (int sy = -1; sy <= 1; sy++)
+#pragma unroll
+        for (int sx = -1; sx <= 1; sx++) {
+          const float ws = (sx == 0 ? 0.5f : 0.25f) * (sy == 0 ? 0.5f : 0.25f);
+          const int h = (hx + sx) + HALO_X * ((hy + sy) + HALO_Y * (hz0 + pl));
+          px += ws * sm.g[0][h];
+          py += ws * sm.g[1][h];
+          pz += ws * sm.g[2][h];
+        }
+      const float w0 = pl == 0 ? 0.25f : (pl == 1 ? 0.5f : (pl == 2 ? 0.25f : 0.0f));
+      const float w1 = pl == 0 ? 0.0f : (pl == 1 ? 0.25f : (pl == 2 ? 0.5f : 0.25f));
+      if (pl < 3) {
+        sg[0][0] += w0 * px; sg[0][1] += w0 * py; sg[0][2] += w0 * pz;
+      }
+      if (pl > 0) {
+        sg[1][0] += w1 * px; sg[1][1] += w1 * py; sg[1][2] += w1 * pz;
+      }
+    }
+  }
   int nclamp = 0;
 #pragma unroll 1
-  for (int zz = 0; zz < TILE_Z / 2; zz++) {
-    const int z = Z0 + threadIdx.z + 2 * zz;
+  for (int zz = 0; zz < 2; zz++) {
+    const int z = Z0 + 2 * threadIdx.z + zz;
     if (x < 1 || x > g.Nx - 2 || y < 1 || y > g.Ny - 2 || z < 1 || z > g.Nz - 2) continue;
-    const long long i = x + (long long)g.Nx * (y + (long long)g.Ny * z);
+    const int i = x + g.Nx * (y + g.Ny * z);
     float f[19];
     if (FIRST) {
 #pragma unroll
-      for (int q = 0; q < 19; q++) f[q] = __ldg(a.fin + q * NC + i);
+      for (int q = 0; q < 19; q++) f[q] = Stored<ST>::load(fin + q * NC + i, WQ(q));
     } else {
       int dxm, dxp, dym, dyp, dzm, dzp;
       neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
-      gather(f, a.fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp);
+      gather(f, fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp);
       boundaries(f, g, a.p, x, y, z);
     }
-    float gx = a.p.g[0], gy = a.p.g[1], gz = a.p.g[2];
-    if (cnt > 0) {
-      const int hx = x - X0 + 1, hy = y - Y0 + 1, hz = z - Z0 + 1;
-#pragma unroll
-      for (int sx = -1; sx <= 1; sx++)
-#pragma unroll
-        for (int sy = -1; sy <= 1; sy++)
-#pragma unroll
-          for (int sz = -1; sz <= 1; sz++) {
-            const float ws = sten[sx + 1] * sten[sy + 1] * sten[sz + 1];
-            const int h = (hx + sx) + HALO_X * ((hy + sy) + HALO_Y * (hz + sz));
-            gx += ws * sm.g[0][h];
-            gy += ws * sm.g[1][h];
-            gz += ws * sm.g[2][h];
-          }
-    }
+    const float gx = a.p.g[0] + (zz ? sg[1][0] : sg[0][0]);
+    const float gy = a.p.g[1] + (zz ? sg[1][1] : sg[0][1]);
+    const float gz = a.p.g[2] + (zz ? sg[1][2] : sg[0][2]);
     float rho = 0.0f;
 #pragma unroll
     for (int q = 0; q < 19; q++) rho += f[q];
     const float jx = f[1] - f[2] + f[7] + f[8] + f[9] + f[10] - f[11] - f[12] - f[13] - f[14];
     const float jy = f[3] - f[4] + f[7] - f[8] + f[11] - f[12] + f[15] + f[16] - f[17] - f[18];
     const float jz = f[5] - f[6] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16] + f[17] - f[18];
-    const float ux = (jx + 0.5f * gx) / rho, uy = (jy + 0.5f * gy) / rho, uz = (jz + 0.5f * gz) / rho;
+    const float ir = __fdividef(1.0f, rho);
+    const float ux = (jx + 0.5f * gx) * ir, uy = (jy + 0.5f * gy) * ir, uz = (jz + 0.5f * gz) * ir;
     a.u[i] = ux;
     a.u[i + NC] = uy;
     a.u[i + 2 * NC] = uz;
-    if (!(fabsf(ux) + fabsf(uy) + fabsf(uz) < 1e30f) || !(rho > 0.0f)) atomicOr(a.err, ERR_NONFINITE);
+    // A non-finite population makes rho non-finite; a vanishing or negative
+    // density is flagged too.
+    if (!(rho > 0.0f && rho < 1e30f)) atomicOr(a.err, ERR_NONFINITE);
     float tau = VAR ? a.tau[i] : a.p.tauN;
     bool clamped = false;
-    collide<COLL, VAR>(f, rho, ux, uy, uz, gx, gy, gz, tau, a.p, clamped);
+    collide<COLL, VAR>(f, rho, ir, ux, uy, uz, gx, gy, gz, tau, a.p, clamped);
     if (VAR) {
       a.tau[i] = tau;
       nclamp += clamped ? 1 : 0;
     }
 #pragma unroll
-    for (int q = 0; q < 19; q++) a.fout[q * NC + i] = f[q];
+    for (int q = 0; q < 19; q++) Stored<ST>::store(fout + q * NC + i, f[q], WQ(q));
   }
   if (VAR && nclamp) atomicAdd(a.clamps, (unsigned long long)nclamp);
 }
 
 // Post-streaming, post-boundary populations of the last step (what the
 // reference's f_s holds after its boundary kernels), for read-back.
+template <typename ST>
 __global__ void materialize_f_kernel(const FluidArgs a, float* __restrict__ out) {
   const Geom& g = a.g;
   const long long NC = g.NC;
@@ -554,11 +633,11 @@ __global__ void materialize_f_kernel(const FluidArgs a, float* __restrict__ out)
     const int x = 1 + (int)(k % (g.Nx - 2));
     const int y = 1 + (int)((k / (g.Nx - 2)) % (g.Ny - 2));
     const int z = 1 + (int)(k / ((long long)(g.Nx - 2) * (g.Ny - 2)));
-    const long long i = x + (long long)g.Nx * (y + (long long)g.Ny * z);
+    const int i = x + g.Nx * (y + g.Ny * z);
     int dxm, dxp, dym, dyp, dzm, dzp;
     neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
     float f[19];
-    gather(f, a.fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp);
+    gather(f, static_cast<const ST*>(a.fin), NC, i, dxm, dxp, dym, dyp, dzm, dzp);
     boundaries(f, g, a.p, x, y, z);
 #pragma unroll
     for (int q = 0; q < 19; q++) out[q * NC + i] = f[q];
@@ -615,6 +694,23 @@ struct Kin {
   float4 x, v, q, w;
 };
 
+__device__ __forceinline__ Kin load_kin(const float4* __restrict__ kin, int p, int np) {
+  Kin k;
+  k.x = kin[p];
+  k.v = kin[p + np];
+  k.q = kin[p + 2 * np];
+  k.w = kin[p + 3 * np];
+  return k;
+}
+
+// fmodf(a, w) for w > 0: a itself for 0 <= a < w, a - w (exact: Sterbenz)
+// for w <= a < 2w, the library function otherwise.  Bit-identical to fmodf.
+__device__ __forceinline__ float wrap_mod(float a, float w) {
+  if (a >= 0.0f && a < w) return a;
+  if (a >= w && a < 2.0f * w) return __fsub_rn(a, w);
+  return fmodf(a, w);
+}
+
 // particle_dynamics for one sphere (CPU_program.cl:209-276).
 __device__ Kin rigid_update(const ParticleArgs& a, int p) {
   const ParticleParams& P = a.p;
@@ -641,7 +737,7 @@ __device__ Kin rigid_update(const ParticleArgs& a, int p) {
   const float4 rt = f4add(f4add(k.x, k.v), f4mul(acc, 0.5f));
   const float4 rw = f4add(rt, W);
   Kin o;
-  o.x = make_float4(fmodf(rw.x, W.x), fmodf(rw.y, W.y), fmodf(rw.z, W.z), fmodf(rw.w, W.w));
+  o.x = make_float4(wrap_mod(rw.x, W.x), wrap_mod(rw.y, W.y), wrap_mod(rw.z, W.z), wrap_mod(rw.w, W.w));
   o.v = f4add(k.v, acc);
   const float dqw = -__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(k.w.x, k.q.x), __fmul_rn(k.w.y, k.q.y)),
                                          __fmul_rn(k.w.z, k.q.z)),
@@ -716,8 +812,7 @@ __device__ bool pair_force(const ParticleParams& P, const Kin& A, const Kin& B, 
   return any;
 }
 
-// One block per reference work-group of markers (blocks [0, np*nfa)), then
-// blocks of warps for the particle-particle forces, one warp per sphere.
+// One block per reference work-group of markers (np*nfa blocks).
 __global__ void particle_step_kernel(const ParticleArgs a) {
   extern __shared__ float4 red[];  // [2*blockDim.x]: forces, then torques
   const ParticleParams& P = a.p;
@@ -744,7 +839,7 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
       const float4 r0 = a.sphere[pt];
       const float4 W = make_float4(P.S[0], P.S[1], P.S[2], 1.0f);
       const float4 rw = f4add(f4add(k.x, r0), W);
-      const float4 rpp = make_float4(fmodf(rw.x, W.x), fmodf(rw.y, W.y), fmodf(rw.z, W.z), fmodf(rw.w, W.w));
+      const float4 rpp = make_float4(wrap_mod(rw.x, W.x), wrap_mod(rw.y, W.y), wrap_mod(rw.z, W.z), wrap_mod(rw.w, W.w));
       const float fx = floorf(rpp.x), fy = floorf(rpp.y), fz = floorf(rpp.z);
       const int x0 = (int)fx + P.buffer[0], y0 = (int)fy + P.buffer[1], z0 = (int)fz + P.buffer[2];
       const bool ok = fx == fx && fy == fy && fz == fz && x0 >= 1 && x0 <= g.Nx - 2 && y0 >= 1 &&
@@ -785,24 +880,39 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
     }
     // List the marker in every fluid tile whose halo holds one of its
     // stencil nodes; lanes inserting into the same tile share one atomic.
+    // All atomics of the warp are issued before any result is used, so
+    // their round trips overlap.
     {
       const int n = nx * ny * nz;
       int nmax = n;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
-      for (int j = 0; j < nmax; j++) {
+      int tileOf[8], baseOf[8];
+      unsigned peersOf[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        tileOf[j] = -1;
+        baseOf[j] = 0;
+        peersOf[j] = 0u;
+        if (j >= nmax) continue;
         const bool act = j < n;
         const unsigned amask = __ballot_sync(0xffffffffu, act);
         if (act) {
           const int ia = j % nx, ib = (j / nx) % ny, ic = j / (nx * ny);
           const int T = tx[ia] + g.ntx * (ty[ib] + g.nty * tz[ic]);
           const unsigned peers = __match_any_sync(amask, T);
-          const int leader = __ffs(peers) - 1;
-          int base = 0;
-          if (lane == leader) base = atomicAdd(&a.tiles.count[T], __popc(peers));
-          base = __shfl_sync(peers, base, leader);
-          const int slot = base + __popc(peers & ((1u << lane) - 1u));
-          if (slot < a.tiles.cap) a.tiles.list[(long long)T * a.tiles.cap + slot] = (int)gid;
+          tileOf[j] = T;
+          peersOf[j] = peers;
+          if (lane == __ffs(peers) - 1) baseOf[j] = atomicAdd(&a.tiles.count[T], __popc(peers));
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        if (j >= nmax) continue;
+        const int base = __shfl_sync(0xffffffffu, baseOf[j], peersOf[j] ? __ffs(peersOf[j]) - 1 : lane);
+        if (tileOf[j] >= 0) {
+          const int slot = base + __popc(peersOf[j] & ((1u << lane) - 1u));
+          if (slot < a.tiles.cap) a.tiles.list[(long long)tileOf[j] * a.tiles.cap + slot] = (int)gid;
           else atomicOr(a.err, ERR_TILE_OVERFLOW);
         }
       }
@@ -836,16 +946,25 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
     return;
   }
 
-  // Particle-particle forces (CPU_program.cl:76-184), one warp per sphere pi:
-  // every pair occurrence the reference's zone loops produce for pi, as the
+}
+
+// Particle-particle forces (CPU_program.cl:76-184) from the positions the
+// particle pass of this step wrote, after it (the reference's order:
+// particle_dynamics, IBM, particle_particle_forces).  One warp per sphere pi.
+__global__ void contact_kernel(const ParticleArgs a) {
+  const ParticleParams& P = a.p;
+  const int np = P.np;
+  const int l = threadIdx.x;
+  const int lane = l & 31;
+  // Every pair occurrence the reference's zone loops produce for pi: as the
   // higher index (neighbour zones of pi's zone, members pj < pi; lane t takes
   // neighbour entry t) and as the lower one (zones whose neighbour list names
   // pi's zone, members pk > pi; lanes over the reverse table), then a fixed
   // shuffle reduction: deterministic.
-  const int pi = (blockIdx.x - ngroups) * (blockDim.x / 32) + (l >> 5);
+  const int pi = blockIdx.x * (blockDim.x / 32) + (l >> 5);
   if (pi >= np) return;  // whole warps
   const int nzones = P.numZones[0] * P.numZones[1] * P.numZones[2];
-  const Kin ki = rigid_update(a, pi);
+  const Kin ki = load_kin(a.kin_new, pi, np);
   float4 F = make_float4(0.f, 0.f, 0.f, 0.f);
   const int pz = a.parsZone[pi];
   if (P.exact) {
@@ -860,7 +979,7 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
         for (int j = 0; j < a.numParInZone[zid]; j++) {
           const int pj = a.zoneMembers[zid * np + j];
           if (!(pi > pj)) continue;
-          const Kin kj = rigid_update(a, pj);
+          const Kin kj = load_kin(a.kin_new, pj, np);
           float4 e;
           float fm;
           if (pair_force(P, ki, kj, e, fm)) F = f4sub(F, f4mul(e, fm));
@@ -880,7 +999,7 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
         for (int t = 1; t <= a.znd[28 * Y]; t++) {
           if (a.znd[28 * Y + t] != pz) continue;
           if (!have) {
-            kk = rigid_update(a, pk);
+            kk = load_kin(a.kin_new, pk, np);
             have = true;
           }
           float4 e;
@@ -902,7 +1021,7 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
       for (int j = 0; j < cnt; j++) {
         const int pj = a.zoneMembers[zid * np + j];
         if (!(pi > pj)) continue;
-        const Kin kj = rigid_update(a, pj);
+        const Kin kj = load_kin(a.kin_new, pj, np);
         float4 e;
         float fm;
         if (pair_force(P, ki, kj, e, fm)) F = f4sub(F, f4mul(e, fm));
@@ -914,7 +1033,7 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
       for (int j = 0; j < cnt; j++) {
         const int pk = a.zoneMembers[Y * np + j];
         if (!(pk > pi)) continue;
-        const Kin kk = rigid_update(a, pk);
+        const Kin kk = load_kin(a.kin_new, pk, np);
         float4 e;
         float fm;
         if (pair_force(P, kk, ki, e, fm)) F = f4add(F, f4mul(e, fm));
@@ -937,6 +1056,7 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
   a.pf_new[pi] = F;
   a.pf_new[pi + np] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
+
 
 // update_particle_zones (CPU_program.cl:280-315) for all spheres: members of
 // each zone listed in increasing sphere index, the order the reference's
@@ -975,37 +1095,83 @@ __global__ void marker_cells_kernel(const float4* mrec, int M, int* cells) {
   cells[3 * m + 2] = z0;
 }
 
+// Float distributions <-> stored form, element by element (row q of the
+// 19 x N_C array carries the shift w_q).
+template <typename ST>
+__global__ void store_f_kernel(const float* __restrict__ in, ST* __restrict__ out, long long NC) {
+  const long long n = 19 * NC;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(k / NC);
+    Stored<ST>::store(out + k, in[k], q == 0 ? WQ(0) : (q <= 6 ? WQ(1) : WQ(7)));
+  }
+}
+
+template <typename ST>
+__global__ void load_f_kernel(const ST* __restrict__ in, float* __restrict__ out, long long NC) {
+  const long long n = 19 * NC;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(k / NC);
+    out[k] = Stored<ST>::load(in + k, q == 0 ? WQ(0) : (q <= 6 ? WQ(1) : WQ(7)));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Launchers.
-template <bool FIRST, bool VAR, int COLL>
+template <bool FIRST, bool VAR, int COLL, typename ST>
 static cudaError_t launch_fluid_t(const FluidArgs& a, cudaStream_t s) {
   dim3 block(TILE_X, TILE_Y, 2);
   dim3 grid(a.g.ntx, a.g.nty, a.g.ntz);
-  fluid_step_kernel<FIRST, VAR, COLL><<<grid, block, 0, s>>>(a);
+  fluid_step_kernel<FIRST, VAR, COLL, ST><<<grid, block, 0, s>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_fluid(const FluidArgs& a, bool first, bool variable, int collision, cudaStream_t s) {
+template <typename ST>
+static cudaError_t launch_fluid_st(const FluidArgs& a, bool first, bool variable, int collision, cudaStream_t s) {
   if (collision == 0) {
-    if (first) return variable ? launch_fluid_t<true, true, 0>(a, s) : launch_fluid_t<true, false, 0>(a, s);
-    return variable ? launch_fluid_t<false, true, 0>(a, s) : launch_fluid_t<false, false, 0>(a, s);
+    if (first) return variable ? launch_fluid_t<true, true, 0, ST>(a, s) : launch_fluid_t<true, false, 0, ST>(a, s);
+    return variable ? launch_fluid_t<false, true, 0, ST>(a, s) : launch_fluid_t<false, false, 0, ST>(a, s);
   }
-  if (first) return variable ? launch_fluid_t<true, true, 1>(a, s) : launch_fluid_t<true, false, 1>(a, s);
-  return variable ? launch_fluid_t<false, true, 1>(a, s) : launch_fluid_t<false, false, 1>(a, s);
+  if (first) return variable ? launch_fluid_t<true, true, 1, ST>(a, s) : launch_fluid_t<true, false, 1, ST>(a, s);
+  return variable ? launch_fluid_t<false, true, 1, ST>(a, s) : launch_fluid_t<false, false, 1, ST>(a, s);
 }
 
-cudaError_t launch_materialize_f(const FluidArgs& a, float* out, cudaStream_t s) {
-  materialize_f_kernel<<<1184, 256, 0, s>>>(a, out);
+cudaError_t launch_fluid(const FluidArgs& a, bool first, bool variable, int collision, int storage, cudaStream_t s) {
+  if (storage == STORE_F16) return launch_fluid_st<__half>(a, first, variable, collision, s);
+  if (storage == STORE_BF16) return launch_fluid_st<__nv_bfloat16>(a, first, variable, collision, s);
+  return launch_fluid_st<float>(a, first, variable, collision, s);
+}
+
+cudaError_t launch_materialize_f(const FluidArgs& a, int storage, float* out, cudaStream_t s) {
+  if (storage == STORE_F16) materialize_f_kernel<__half><<<1184, 256, 0, s>>>(a, out);
+  else if (storage == STORE_BF16) materialize_f_kernel<__nv_bfloat16><<<1184, 256, 0, s>>>(a, out);
+  else materialize_f_kernel<float><<<1184, 256, 0, s>>>(a, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_store_f(const float* in, void* out, long long NC, int storage, cudaStream_t s) {
+  if (storage == STORE_F16) store_f_kernel<__half><<<1184, 256, 0, s>>>(in, static_cast<__half*>(out), NC);
+  else if (storage == STORE_BF16)
+    store_f_kernel<__nv_bfloat16><<<1184, 256, 0, s>>>(in, static_cast<__nv_bfloat16*>(out), NC);
+  else store_f_kernel<float><<<1184, 256, 0, s>>>(in, static_cast<float*>(out), NC);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_load_f(const void* in, float* out, long long NC, int storage, cudaStream_t s) {
+  if (storage == STORE_F16) load_f_kernel<__half><<<1184, 256, 0, s>>>(static_cast<const __half*>(in), out, NC);
+  else if (storage == STORE_BF16)
+    load_f_kernel<__nv_bfloat16><<<1184, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(in), out, NC);
+  else load_f_kernel<float><<<1184, 256, 0, s>>>(static_cast<const float*>(in), out, NC);
   return cudaGetLastError();
 }
 
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s) {
   const int ngroups = a.p.np * a.p.nfa;
   const int threads = a.p.L < 128 ? 128 : a.p.L;
-  const int warps = threads / 32;
-  const int ppblocks = (a.p.np + warps - 1) / warps;
   const size_t smem = sizeof(float4) * 2 * threads;
-  particle_step_kernel<<<ngroups + ppblocks, threads, smem, s>>>(a);
+  particle_step_kernel<<<ngroups, threads, smem, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  contact_kernel<<<(a.p.np + 3) / 4, 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 
