@@ -6,6 +6,7 @@
 
 Usage: python build.py [--force]
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -48,7 +49,7 @@ def build(force: bool = False, verbose_ptxas: bool = False):
     os.makedirs(BIN, exist_ok=True)
     if force or _stale(CUDA_LIB, CU_SRC + CU_HDR + [__file__]):
         os.makedirs(OBJ, exist_ok=True)
-        objs = []
+        objs, cmds = [], []
         for src in CU_SRC:
             obj = os.path.join(OBJ, os.path.basename(src) + ".o")
             cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-c", "-o", obj, src]
@@ -56,8 +57,11 @@ def build(force: bool = False, verbose_ptxas: bool = False):
                 cmd.insert(1, "--fmad=false")
             if verbose_ptxas:
                 cmd.insert(1, "-Xptxas=-v")
-            _run(cmd)
+            cmds.append(cmd)
             objs.append(obj)
+        # The translation units are independent: compile them concurrently.
+        with concurrent.futures.ThreadPoolExecutor(max_workers=len(cmds)) as ex:
+            list(ex.map(_run, cmds))
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", CUDA_LIB] + objs)
     if force or _stale(HOST_LIB, HOST_SRC + HOST_HDR + [__file__]):
         _run(["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-Wall", "-Wno-unused-result", "-o", HOST_LIB]

@@ -26,6 +26,13 @@ struct d3q19_ctx {
   d3q19_options opt;
   int dev = 0;
   cudaStream_t stream = nullptr;
+  // The particle-particle forces and the zone rebuild of step t feed only
+  // the rigid-body update of step t+1: they run on a second stream, forked
+  // after the particle pass and joined before the next one, so that the
+  // collide of step t+1 overlaps them.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool side_pending = false;
   Geom g;
   FluidParams fpar;
   ParticleParams ppar;
@@ -184,9 +191,12 @@ extern "C" int d3q19_create(const int_param_struct* ip, const flp_param_struct* 
   c->opt = o;
   c->dev = o.device;
   cudaSetDevice(c->dev);
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    delete c;
-    return fail(nullptr, D3Q19_ECUDA, "cudaStreamCreate failed");
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    d3q19_destroy(c);
+    return fail(nullptr, D3Q19_ECUDA, "stream or event creation failed");
   }
   Geom& g = c->g;
   g.Nx = ip->LatticeSize[0];
@@ -532,6 +542,8 @@ static int enqueue_step(d3q19_ctx* c, int t) {
     pa.revList = c->revList;
     pa.err = c->err;
     pa.t = t;
+    // The rigid-body update reads the contact forces of step t-1.
+    if (c->side_pending) CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     if (c->profiling) {
       CUDA_TRY(c, cudaEventCreate(&e0));
       CUDA_TRY(c, cudaEventCreate(&e1));
@@ -542,6 +554,12 @@ static int enqueue_step(d3q19_ctx* c, int t) {
       CUDA_TRY(c, cudaEventRecord(e1, c->stream));
       c->ev_part.emplace_back(e0, e1);
     }
+    // Contacts from the positions just written, then (when due) the zone
+    // lists the contacts of step t+1 use, on the side stream
+    // (sim_main.c:410-447: particle_particle_forces, update_particle_zones).
+    CUDA_TRY(c, cudaEventRecord(c->ev_fork, c->stream));
+    CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    CUDA_TRY(c, launch_contacts(pa, c->side));
     c->pcur = 1 - c->pcur;
     if (t % c->opt.rebuild_freq == 0) {
       ZoneArgs za;
@@ -552,10 +570,21 @@ static int enqueue_step(d3q19_ctx* c, int t) {
       za.numParInZone = c->numParInZone;
       za.zoneOf = c->zoneOf;
       za.err = c->err;
-      CUDA_TRY(c, launch_zones(za, c->stream));
+      CUDA_TRY(c, launch_zones(za, c->side));
     }
+    CUDA_TRY(c, cudaEventRecord(c->ev_join, c->side));
+    c->side_pending = true;
   }
   c->last_t = t;
+  return 0;
+}
+
+// Orders the side stream's pending work (contacts, zone rebuild) before
+// whatever the main stream runs next.
+static int join_side(d3q19_ctx* c) {
+  if (!c->side_pending) return 0;
+  CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+  c->side_pending = false;
   return 0;
 }
 
@@ -563,7 +592,8 @@ extern "C" int d3q19_step(d3q19_ctx* c, int t) {
   int rc = check_ready(c);
   if (rc) return rc;
   cudaSetDevice(c->dev);
-  return enqueue_step(c, t);
+  if ((rc = enqueue_step(c, t))) return rc;
+  return join_side(c);
 }
 
 static int gcd_i(int a, int b) { return b ? gcd_i(b, a % b) : a; }
@@ -586,17 +616,19 @@ extern "C" int d3q19_run(d3q19_ctx* c, int t0, int nsteps) {
       n--;
       continue;
     }
+    if ((rc = join_side(c))) return rc;
     auto key = std::make_tuple(((t % Lp) + Lp) % Lp, c->cur, c->pcur, CH);
     auto it = c->graphs.find(key);
     if (it == c->graphs.end()) {
       const int cur0 = c->cur, pcur0 = c->pcur;
       cudaGraph_t graph;
       CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      for (int k = 0; k < CH; k++) {
-        if ((rc = enqueue_step(c, t + k))) {
-          cudaStreamEndCapture(c->stream, &graph);
-          return rc;
-        }
+      for (int k = 0; k < CH && !rc; k++) rc = enqueue_step(c, t + k);
+      if (!rc) rc = join_side(c);
+      if (rc) {
+        cudaStreamEndCapture(c->stream, &graph);
+        c->side_pending = false;
+        return rc;
       }
       CUDA_TRY(c, cudaStreamEndCapture(c->stream, &graph));
       cudaGraphExec_t exec;
@@ -611,7 +643,7 @@ extern "C" int d3q19_run(d3q19_ctx* c, int t0, int nsteps) {
     t += CH;
     n -= CH;
   }
-  return 0;
+  return join_side(c);
 }
 
 static int device_errors(d3q19_ctx* c) {
@@ -630,6 +662,7 @@ static int device_errors(d3q19_ctx* c) {
 extern "C" int d3q19_synchronize(d3q19_ctx* c) {
   if (!c) return D3Q19_EINVAL;
   cudaSetDevice(c->dev);
+  if (int rc = join_side(c)) return rc;
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return device_errors(c);
 }
@@ -638,6 +671,7 @@ template <typename T>
 static int readback(d3q19_ctx* c, T* dst, const T* src, size_t n) {
   if (!c || !dst) return D3Q19_EINVAL;
   cudaSetDevice(c->dev);
+  if (int rc = join_side(c)) return rc;
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   CUDA_TRY(c, cudaMemcpy(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost));
   return device_errors(c);
@@ -799,6 +833,7 @@ extern "C" int d3q19_destroy(d3q19_ctx* c) {
   if (!c) return D3Q19_EINVAL;
   cudaSetDevice(c->dev);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->side) cudaStreamSynchronize(c->side);
   for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
   drop_events(c);
   void* ptrs[] = {c->f[0], c->f[1], c->u, c->tau, c->kin[0], c->kin[1], c->pff[0], c->pff[1], c->pf[0], c->pf[1],
@@ -807,6 +842,9 @@ extern "C" int d3q19_destroy(d3q19_ctx* c) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->side) cudaStreamDestroy(c->side);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   delete c;
   return 0;
 }

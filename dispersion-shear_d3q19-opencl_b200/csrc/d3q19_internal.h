@@ -18,6 +18,7 @@ constexpr int HALO_X = TILE_X + 2;
 constexpr int HALO_Y = TILE_Y + 2;
 constexpr int HALO_Z = TILE_Z + 2;
 constexpr int HALO_N = HALO_X * HALO_Y * HALO_Z;
+constexpr int TILE_N = TILE_X * TILE_Y * TILE_Z;
 
 // The spread force is accumulated in fixed point (deterministic: integer sums
 // do not depend on the order markers are visited in).  A contribution v,
@@ -144,7 +145,10 @@ cudaError_t launch_materialize_f(const FluidArgs& a, int storage, float* out, cu
 // row q of each N_C-long row block shifted by w_q).
 cudaError_t launch_store_f(const float* in, void* out, long long NC, int storage, cudaStream_t s);
 cudaError_t launch_load_f(const void* in, float* out, long long NC, int storage, cudaStream_t s);
+// The particle pass (rigid bodies, IBM interpolation and marker lists) and
+// the particle-particle forces from the positions it wrote.
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s);
+cudaError_t launch_contacts(const ParticleArgs& a, cudaStream_t s);
 cudaError_t launch_zones(const ZoneArgs& a, cudaStream_t s);
 cudaError_t launch_spread_field(const Geom& g, const TileLists& t, int last_step, float* out, unsigned* err,
                                 cudaStream_t s);

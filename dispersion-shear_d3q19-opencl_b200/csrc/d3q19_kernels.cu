@@ -64,23 +64,30 @@ namespace d3q19 {
 
 template <typename ST>
 struct Stored;
+// load/store take and give f_q; load_dev/store_dev the deviation f_q - w_q.
 template <>
 struct Stored<float> {
   static __device__ __forceinline__ float load(const float* p, float) { return __ldg(p); }
   static __device__ __forceinline__ void store(float* p, float v, float) { *p = v; }
+  static __device__ __forceinline__ float load_dev(const float* p, float w) { return __ldg(p) - w; }
+  static __device__ __forceinline__ void store_dev(float* p, float d, float w) { *p = d + w; }
 };
 template <>
 struct Stored<__half> {
-  static __device__ __forceinline__ float load(const __half* p, float w) {
-    return __half2float(__ushort_as_half(__ldg(reinterpret_cast<const unsigned short*>(p)))) + w;
+  static __device__ __forceinline__ float load_dev(const __half* p, float) {
+    return __half2float(__ushort_as_half(__ldg(reinterpret_cast<const unsigned short*>(p))));
   }
+  static __device__ __forceinline__ void store_dev(__half* p, float d, float) { *p = __float2half_rn(d); }
+  static __device__ __forceinline__ float load(const __half* p, float w) { return load_dev(p, w) + w; }
   static __device__ __forceinline__ void store(__half* p, float v, float w) { *p = __float2half_rn(v - w); }
 };
 template <>
 struct Stored<__nv_bfloat16> {
-  static __device__ __forceinline__ float load(const __nv_bfloat16* p, float w) {
-    return __bfloat162float(__ushort_as_bfloat16(__ldg(reinterpret_cast<const unsigned short*>(p)))) + w;
+  static __device__ __forceinline__ float load_dev(const __nv_bfloat16* p, float) {
+    return __bfloat162float(__ushort_as_bfloat16(__ldg(reinterpret_cast<const unsigned short*>(p))));
   }
+  static __device__ __forceinline__ void store_dev(__nv_bfloat16* p, float d, float) { *p = __float2bfloat16_rn(d); }
+  static __device__ __forceinline__ float load(const __nv_bfloat16* p, float w) { return load_dev(p, w) + w; }
   static __device__ __forceinline__ void store(__nv_bfloat16* p, float v, float w) {
     *p = __float2bfloat16_rn(v - w);
   }
@@ -92,7 +99,11 @@ struct Stored<__nv_bfloat16> {
 // inward normal +A; SIDE 1 = upper), rho = 1, the inward normal velocity
 // follows from the knowns, and each unknown is its opposite population plus
 // rho*(u_n + c_t.u_t)/6, or rho*u_n/3 for the normal direction.
-template <int A, int SIDE>
+// DEV: f holds deviations from the rest state, f_q - w_q (the weights of the
+// 9 tangential and the 5 outgoing populations sum to 2/3 and 1/6, so
+// 1 - (sum9 + 2 sum5) becomes -(sum9 + 2 sum5); unknown and opposite
+// population share w_q).
+template <int A, int SIDE, bool DEV = false>
 __device__ __forceinline__ void velocity_bc(float (&f)[19], const float* uw) {
   constexpr int IN = SIDE == 0 ? 1 : -1;
   constexpr int A1 = A == 0 ? 1 : 0;
@@ -104,7 +115,7 @@ __device__ __forceinline__ void velocity_bc(float (&f)[19], const float* uw) {
     else if (CAQ(A, q) == -IN) sum5 += f[q];
   }
   const float rho = 1.0f;
-  const float un = 1.0f - (sum9 + 2.0f * sum5) / rho;
+  const float un = DEV ? -(sum9 + 2.0f * sum5) : 1.0f - (sum9 + 2.0f * sum5) / rho;
   const float ua1 = uw[A1], ua2 = uw[A2];
 #pragma unroll
   for (int q = 1; q < 19; q++) {
@@ -122,14 +133,15 @@ __device__ __forceinline__ void velocity_bc(float (&f)[19], const float* uw) {
   }
 }
 
+template <bool DEV = false>
 __device__ __forceinline__ void apply_wall(float (&f)[19], int axis, int side, const FluidParams& p) {
   const float* uw = side ? p.velUpper : p.velLower;
   if (axis == 0) {
-    if (side) velocity_bc<0, 1>(f, uw); else velocity_bc<0, 0>(f, uw);
+    if (side) velocity_bc<0, 1, DEV>(f, uw); else velocity_bc<0, 0, DEV>(f, uw);
   } else if (axis == 1) {
-    if (side) velocity_bc<1, 1>(f, uw); else velocity_bc<1, 0>(f, uw);
+    if (side) velocity_bc<1, 1, DEV>(f, uw); else velocity_bc<1, 0, DEV>(f, uw);
   } else {
-    if (side) velocity_bc<2, 1>(f, uw); else velocity_bc<2, 0>(f, uw);
+    if (side) velocity_bc<2, 1, DEV>(f, uw); else velocity_bc<2, 0, DEV>(f, uw);
   }
 }
 
@@ -137,10 +149,14 @@ __device__ __forceinline__ void apply_wall(float (&f)[19], int axis, int side, c
 // approximations of the reciprocal, reciprocal square root and power
 // (a few ulp; the reference-exact arithmetic evaluates them as written).
 // Optional extensions: an upper clamp and a regularised Casson yield term.
+// VISC is the viscosity law fixed at compile time (2 power law, 3
+// Herschel-Bulkley, 4 Casson), or -1 to read it from p.viscModel.
+template <int VISC = -1>
 __device__ __forceinline__ float compute_tau(const FluidParams& p, float srt, bool& clamped) {
   float tau = p.tauN;
   const float eps = 1e-8f;
-  if (p.viscModel == 2) {  // power law
+  const int model = VISC >= 0 ? VISC : p.viscModel;
+  if (model == 2) {  // power law
     float k = p.visc[0], n = p.visc[1], nu;
     srt = srt > eps ? srt : eps;
     if (n == 0.5f) nu = k * rsqrtf(srt);
@@ -148,13 +164,13 @@ __device__ __forceinline__ float compute_tau(const FluidParams& p, float srt, bo
     else if (n == 2.0f) nu = k * srt;
     else nu = k * exp2f(__log2f(srt) * (n - 1.0f));
     tau = 3.0f * nu + 0.5f;
-  } else if (p.viscModel == 4) {  // Casson
+  } else if (model == 4) {  // Casson
     float tY = p.visc[0], eta = p.visc[1];
     srt = srt > eps ? srt : eps;
     float sr2 = p.cassonReg > 0.0f ? srt * srt + p.cassonReg * p.cassonReg : srt * srt;
     float a = sqrtf(tY * rsqrtf(sr2)) + sqrtf(eta);
     tau = 3.0f * (a * a) + 0.5f;
-  } else if (p.viscModel == 3) {  // Herschel-Bulkley
+  } else if (model == 3) {  // Herschel-Bulkley
     float tY = p.visc[0], k = p.visc[1], n = p.visc[2], nu;
     srt = srt > eps ? srt : eps;
     const float yield = __fdividef(tY, srt);
@@ -190,7 +206,7 @@ __device__ __forceinline__ float compute_tau(const FluidParams& p, float srt, bo
 // Addressing: row q of the distributions starts at fin + q*NC (a 64-bit
 // offset, the same for every thread); within a row the node index is a
 // 32-bit int (N_C < 2^31 is checked when the context is created).
-template <typename ST>
+template <typename ST, bool DEV = false>
 __device__ __forceinline__ void gather(float (&f)[19], const ST* __restrict__ fin, long long NC, int i, int dxm,
                                        int dxp, int dym, int dyp, int dzm, int dzp) {
 #pragma unroll
@@ -198,7 +214,7 @@ __device__ __forceinline__ void gather(float (&f)[19], const ST* __restrict__ fi
     const int cx = CXQ(q), cy = CYQ(q), cz = CZQ(q);
     const int src = i + (cx == 1 ? dxm : (cx == -1 ? dxp : 0)) + (cy == 1 ? dym : (cy == -1 ? dyp : 0)) +
                     (cz == 1 ? dzm : (cz == -1 ? dzp : 0));
-    f[q] = Stored<ST>::load(fin + q * NC + src, WQ(q));
+    f[q] = DEV ? Stored<ST>::load_dev(fin + q * NC + src, WQ(q)) : Stored<ST>::load(fin + q * NC + src, WQ(q));
   }
 }
 
@@ -216,19 +232,20 @@ __device__ __forceinline__ void neighbour_deltas(const Geom& g, int x, int y, in
 
 // Boundary rebuild after the gather: the wall plane of the wall axis, then
 // the tangential velocity boundaries in axis order (sim_main.c:383-402).
+template <bool DEV = false>
 __device__ __forceinline__ void boundaries(float (&f)[19], const Geom& g, const FluidParams& p, int x, int y,
                                            int z) {
   if (g.wallAxis < 0) return;
   const int c[3] = {x, y, z};
   const int N[3] = {g.Nx, g.Ny, g.Nz};
   const int a = g.wallAxis;
-  if (c[a] == 1) apply_wall(f, a, 0, p);
-  else if (c[a] == N[a] - 2) apply_wall(f, a, 1, p);
+  if (c[a] == 1) apply_wall<DEV>(f, a, 0, p);
+  else if (c[a] == N[a] - 2) apply_wall<DEV>(f, a, 1, p);
 #pragma unroll
   for (int t = 0; t < 3; t++) {
     if (!g.tanBC[t]) continue;
-    if (c[t] == 1) apply_wall(f, t, 0, p);
-    else if (c[t] == N[t] - 2) apply_wall(f, t, 1, p);
+    if (c[t] == 1) apply_wall<DEV>(f, t, 0, p);
+    else if (c[t] == N[t] - 2) apply_wall<DEV>(f, t, 1, p);
   }
 }
 
@@ -254,8 +271,9 @@ __device__ __forceinline__ void boundaries(float (&f)[19], const Geom& g, const 
 // every step, as the reference does, instead of letting that rounding
 // difference accumulate as a momentum drift.  COLL 0: the reference's rate
 // vector with 1/tau at rows 8,9,10,14,15 (GPU_program.cl:453, 567-568);
-// COLL 1: BGK.
-template <int COLL, bool VAR>
+// COLL 1: BGK.  VISC 0: constant tau; otherwise the local tau of viscosity
+// law VISC (1 Newtonian, 2 power law, 3 Herschel-Bulkley, 4 Casson).
+template <int COLL, int VISC>
 __device__ __forceinline__ void collide(float (&f)[19], float rho, float ir, float ux, float uy, float uz, float gx,
                                         float gy, float gz, float& tau, const FluidParams& p, bool& clamped) {
   // Equilibrium minus f, pairwise (GPU_program.cl:978-1007), and the Guo term
@@ -339,7 +357,7 @@ __device__ __forceinline__ void collide(float (&f)[19], float rho, float ir, flo
     s1 = 1.19f; s2 = 1.40f; s4 = 1.20f; s6 = 1.20f; s11 = 1.20f; s12 = 1.40f; s13 = 1.40f; s16 = 1.98f;
   }
 
-  if (VAR) {
+  if (VISC != 0) {
     // Strain rate from the relaxed non-equilibrium moments with tau(t-1)
     // (GPU_program.cl:459-562): the second moments of M^-1 S_old M d, which
     // only rows e, 3pxx, pww and the off-diagonal p carry.
@@ -358,7 +376,7 @@ __device__ __forceinline__ void collide(float (&f)[19], float rho, float ir, flo
     const float sxy = 4.0f * a13, syz = 4.0f * a14, sxz = 4.0f * a15;
     const float ss = sxx * sxx + 2.0f * (sxy * sxy + sxz * sxz + syz * syz) + syy * syy + szz * szz;
     const float srt = sqrtf(ss) * 2.1213203f * ir;
-    tau = compute_tau(p, srt, clamped);
+    tau = compute_tau<VISC>(p, srt, clamped);
   }
 
   const float it = __fdividef(1.0f, tau);
@@ -414,12 +432,17 @@ __device__ __forceinline__ void collide(float (&f)[19], float rho, float ir, flo
 // ---------------------------------------------------------------------------
 // Spread force of one tile: accumulate -w*F of every listed marker on the
 // tile plus a one-node halo (the reference's gpf slot sum, GPU_program.cl:
-// 210-227 and 258-289) in 2^-40 fixed point, then convert to float.
+// 210-227 and 258-289) in fixed point, then convert to float.  The 64-bit
+// accumulators and the float field share the storage: the field replaces the
+// sums once they are complete.
 struct __align__(16) SpreadSmem {
-  int hi[3][HALO_N];        // sum of the high parts (v >> 16)
-  unsigned lo[3][HALO_N];   // sum of the low 16 bits
-  float g[3][HALO_N];       // the spread force of the halo nodes
+  union {
+    unsigned long long acc[3][HALO_N];  // fixed-point sums: lo parts (low word), hi parts (high word)
+    float g[3][HALO_N];                 // the spread force of the halo nodes
+  };
 };
+static_assert((3 * HALO_N) % 2 == 0, "the sums are cleared sixteen bytes at a time");
+constexpr int SPREAD_CONVERT_PER_THREAD = (3 * HALO_N + FLUID_THREADS - 1) / FLUID_THREADS;
 
 __device__ __forceinline__ void marker_weights(float wx, float wy, float wz, float (&w)[8]) {
   // GPU_program.cl:170-178.
@@ -450,23 +473,35 @@ __device__ __forceinline__ int fixed_exponent(unsigned fmax_bits) {
   return FIX_BITS - e;
 }
 
-// Accumulates the tile's listed markers into s (X0,Y0,Z0 = tile origin) and
-// leaves the halo's spread force in s.g.  Every contribution -w*F (the
+// Accumulates the tile's n listed markers into s (X0,Y0,Z0 = tile origin)
+// and leaves the halo's spread force in s.g.  Thread t takes list entries
+// t, t + FLUID_THREADS, ...; its first entry (first_id, loaded by the caller
+// ahead of time) is used when t < n.  Every contribution -w*F (the
 // reference's "gpf -= weights[n]*vuForce", GPU_program.cl:222-224) is scaled
-// by 2^k (exact), rounded to an integer and summed exactly in two 32-bit
-// parts; the sum is converted back once.
+// by 2^k (exact), rounded to an integer v = hi*2^16 + lo (0 <= lo < 2^16) and
+// the two parts are summed exactly with 32-bit atomics, lo in the low word and
+// hi in the high word of the node's 64-bit slot; each sum is converted back
+// with one rounding.  Needs all FLUID_THREADS threads.
 __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& tl, long long T, int n, int X0,
-                                int Y0, int Z0, int tid, int nthreads, int k, unsigned* err) {
-  static_assert((3 * HALO_N) % 4 == 0, "halo arrays are cleared and converted four words at a time");
+                                int Y0, int Z0, int tid, int k, int first_id, unsigned* err) {
+  float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
+  if (tid < n) {  // issued before the clear so that the round trip overlaps it
+    ma = tl.mrec[2 * (long long)first_id];
+    mb = tl.mrec[2 * (long long)first_id + 1];
+  }
   {
-    int4* z4 = reinterpret_cast<int4*>(&s.hi[0][0]);  // hi and lo are contiguous
-    for (int h = tid; h < 2 * 3 * HALO_N / 4; h += nthreads) z4[h] = make_int4(0, 0, 0, 0);
+    int4* z4 = reinterpret_cast<int4*>(&s.acc[0][0]);
+    for (int h = tid; h < 3 * HALO_N / 2; h += FLUID_THREADS) z4[h] = make_int4(0, 0, 0, 0);
   }
   __syncthreads();
   const float scale = ldexpf(1.0f, k);
-  for (int j = tid; j < n; j += nthreads) {
-    const int m = tl.list[T * tl.cap + j];
-    const float4 a = tl.mrec[2 * (long long)m], b = tl.mrec[2 * (long long)m + 1];
+  for (int j = tid; j < n; j += FLUID_THREADS) {
+    float4 a = ma, b = mb;
+    if (j != tid) {
+      const int m = tl.list[T * tl.cap + j];
+      a = tl.mrec[2 * (long long)m];
+      b = tl.mrec[2 * (long long)m + 1];
+    }
     int x0, y0, z0;
     decode_marker(a, b, x0, y0, z0);
     const int xs = (x0 == g.Nx - 2) ? -(g.Nx - 3) : 1;
@@ -490,101 +525,144 @@ __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& t
           continue;
         }
         const long long v = __float2ll_rn(sv);
-        atomicAdd(&s.hi[d][h], (int)(v >> 16));
-        atomicAdd(&s.lo[d][h], (unsigned)(v & 0xffff));
+        unsigned* slot = reinterpret_cast<unsigned*>(&s.acc[d][h]);
+        atomicAdd(slot, (unsigned)(v & 0xffff));
+        atomicAdd(reinterpret_cast<int*>(slot + 1), (int)(v >> 16));
       }
     }
   }
   __syncthreads();
   // value = (hi * 2^16 + lo) * 2^-k, both parts scaled exactly by powers of
-  // two and joined with one rounding.
+  // two and joined with one rounding.  All sums are read before the float
+  // field overwrites them.
   const float inv = ldexpf(1.0f, -k), inv_hi = ldexpf(1.0f, 16 - k);
-  {
-    const int4* h4 = reinterpret_cast<const int4*>(&s.hi[0][0]);
-    const uint4* l4 = reinterpret_cast<const uint4*>(&s.lo[0][0]);
-    float4* g4 = reinterpret_cast<float4*>(&s.g[0][0]);
-    for (int h = tid; h < 3 * HALO_N / 4; h += nthreads) {
-      const int4 a = h4[h];
-      const uint4 b = l4[h];
-      g4[h] = make_float4(__fmaf_rn((float)a.x, inv_hi, (float)b.x * inv), __fmaf_rn((float)a.y, inv_hi, (float)b.y * inv),
-                          __fmaf_rn((float)a.z, inv_hi, (float)b.z * inv), __fmaf_rn((float)a.w, inv_hi, (float)b.w * inv));
+  float v[SPREAD_CONVERT_PER_THREAD];
+#pragma unroll
+  for (int r = 0; r < SPREAD_CONVERT_PER_THREAD; r++) {
+    const int h = tid + r * FLUID_THREADS;
+    v[r] = 0.0f;
+    if (h < 3 * HALO_N) {
+      const unsigned* slot = reinterpret_cast<const unsigned*>(&(&s.acc[0][0])[h]);
+      v[r] = __fmaf_rn((float)(int)slot[1], inv_hi, (float)slot[0] * inv);
     }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < SPREAD_CONVERT_PER_THREAD; r++) {
+    const int h = tid + r * FLUID_THREADS;
+    if (h < 3 * HALO_N) (&s.g[0][0])[h] = v[r];
   }
   __syncthreads();
 }
 
-// ---------------------------------------------------------------------------
-template <bool FIRST, bool VAR, int COLL, typename ST>
-__global__ void __launch_bounds__(FLUID_THREADS, 4) fluid_step_kernel(const FluidArgs a) {
-  const ST* __restrict__ fin = static_cast<const ST*>(a.fin);
-  ST* __restrict__ fout = static_cast<ST*>(a.fout);
-  __shared__ SpreadSmem sm;
-  __shared__ int s_cnt;
-  const Geom& g = a.g;
-  const int tid = threadIdx.x + TILE_X * (threadIdx.y + TILE_Y * threadIdx.z);
-  const int nthreads = FLUID_THREADS;
-  const int X0 = blockIdx.x * TILE_X, Y0 = blockIdx.y * TILE_Y, Z0 = blockIdx.z * TILE_Z;
-  const long long T = blockIdx.x + (long long)g.ntx * (blockIdx.y + (long long)g.nty * blockIdx.z);
-
-  int cnt = 0;
-  if (a.has_ibm) {
-    if (tid == 0) s_cnt = a.tiles.count[T];
-    __syncthreads();
-    cnt = s_cnt;
-    // The markers listed now are those of step t-1; the particle pass of
-    // step t records its force maximum in the other slot, cleared here.
-    const unsigned fbits = a.tiles.fmax[(a.t + 1) & 1];
-    if (T == 0 && tid == 0) a.tiles.fmax[a.t & 1] = 0u;
-    if (cnt > 0) {
-      __syncthreads();
-      if (tid == 0) a.tiles.count[T] = 0;  // consumed; the particle pass of this step refills it
-      accumulate_tile(sm, g, a.tiles, T, min(cnt, a.tiles.cap), X0, Y0, Z0, tid, nthreads, fixed_exponent(fbits),
-                      a.err);
+// Smoothed spread force of the tile's 32x4x4 nodes: the reference's
+// 27-point stencil (weights 1/4, 1/2, 1/4 per axis; GPU_program.cl:356-377)
+// over the halo field s.g.  Each thread takes two consecutive z-planes, so the
+// 9-point x-y sums of the two middle halo planes are shared between its nodes.
+__device__ __forceinline__ void smooth_pair(const SpreadSmem& s, int tx, int ty, int tz, float (&sg)[2][3]) {
+  const int hx = tx + 1, hy = ty + 1, hz0 = 2 * tz;
+#pragma unroll
+  for (int pl = 0; pl < 4; pl++) {
+    float px = 0.0f, py = 0.0f, pz = 0.0f;
+#pragma unroll
+    for (int sy = -1; sy <= 1; sy++)
+#pragma unroll
+      for (int sx = -1; sx <= 1; sx++) {
+        const float ws = (sx == 0 ? 0.5f : 0.25f) * (sy == 0 ? 0.5f : 0.25f);
+        const int h = (hx + sx) + HALO_X * ((hy + sy) + HALO_Y * (hz0 + pl));
+        px += ws * s.g[0][h];
+        py += ws * s.g[1][h];
+        pz += ws * s.g[2][h];
+      }
+    const float w0 = pl == 0 ? 0.25f : (pl == 1 ? 0.5f : (pl == 2 ? 0.25f : 0.0f));
+    const float w1 = pl == 0 ? 0.0f : (pl == 1 ? 0.25f : (pl == 2 ? 0.5f : 0.25f));
+    if (pl < 3) {
+      sg[0][0] += w0 * px; sg[0][1] += w0 * py; sg[0][2] += w0 * pz;
+    }
+    if (pl > 0) {
+      sg[1][0] += w1 * px; sg[1][1] += w1 * py; sg[1][2] += w1 * pz;
     }
   }
+}
 
+// Boundary layouts of the collide-stream kernel, fixed at compile time.
+constexpr int BC_GENERIC = 0;  // any combination the context accepts
+constexpr int BC_ZWALL = 1;    // periodic x and y, velocity walls on z, no tangential boundaries
+
+// Dynamic shared memory of the collide-stream kernel: the spread halo of the
+// tile when there are spheres.
+__host__ __device__ constexpr size_t fluid_smem_bytes(bool ibm) { return ibm ? sizeof(SpreadSmem) : 0; }
+
+// Resident blocks per SM the register allocation is sized for (256 threads
+// each).  FP32 storage: 5 (48 registers), 16-bit storage: 4 (64 registers),
+// the faster choices measured on the 128^3 suspension.
+#ifndef FLUID_MIN_BLOCKS_F32
+#define FLUID_MIN_BLOCKS_F32 5
+#endif
+#ifndef FLUID_MIN_BLOCKS
+#define FLUID_MIN_BLOCKS 4
+#endif
+
+// One collide-stream pass over a 32x4x4 tile; each thread takes two
+// consecutive z-planes.  first != 0: the stored state is the reference's
+// post-stream buffer (after an upload), read in place without streaming.
+template <int COLL, int VISC, int BC, typename ST>
+__global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? FLUID_MIN_BLOCKS_F32 : FLUID_MIN_BLOCKS)
+    fluid_step_kernel(const FluidArgs a, const int first) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SpreadSmem& sm = *reinterpret_cast<SpreadSmem*>(smem_raw);
+  const ST* __restrict__ fin = static_cast<const ST*>(a.fin);
+  ST* __restrict__ fout = static_cast<ST*>(a.fout);
+  const Geom& g = a.g;
+  const int tid = threadIdx.x + TILE_X * (threadIdx.y + TILE_Y * threadIdx.z);
+  const int X0 = blockIdx.x * TILE_X, Y0 = blockIdx.y * TILE_Y, Z0 = blockIdx.z * TILE_Z;
+  const int T = blockIdx.x + g.ntx * (blockIdx.y + g.nty * blockIdx.z);
   const int x = X0 + threadIdx.x;
   const int y = Y0 + threadIdx.y;
   const long long NC = g.NC;
-  // Each thread takes two consecutive z-planes, so the 27-point smoothing
-  // (weights 1/4, 1/2, 1/4 per axis) shares the 9-point x-y sums of the two
-  // middle halo planes between its nodes.
+  const bool inxy = x >= 1 && x <= g.Nx - 2 && y >= 1 && y <= g.Ny - 2;
+
+  // IBM force of the tile: the markers listed by the particle pass of step
+  // t-1, accumulated over the tile's halo and smoothed with the reference's
+  // 27-point stencil (GPU_program.cl:356-377), in shared memory only.
   float sg[2][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
-  if (cnt > 0) {
-    const int hx = threadIdx.x + 1, hy = threadIdx.y + 1, hz0 = 2 * threadIdx.z;
-#pragma unroll
-    for (int pl = 0; pl < 4; pl++) {
-      float px = 0.0f, py = 0.0f, pz = 0.0f;
-#pragma unroll
-      for (int sy = -1; sy <= 1; sy++)
-#pragma unroll
-        for (int sx = -1; sx <= 1; sx++) {
-          const float ws = (sx == 0 ? 0.5f : 0.25f) * (sy == 0 ? 0.5f : 0.25f);
-          const int h = (hx + sx) + HALO_X * ((hy + sy) + HALO_Y * (hz0 + pl));
-          px += ws * sm.g[0][h];
-          py += ws * sm.g[1][h];
-          pz += ws * sm.g[2][h];
-        }
-      const float w0 = pl == 0 ? 0.25f : (pl == 1 ? 0.5f : (pl == 2 ? 0.25f : 0.0f));
-      const float w1 = pl == 0 ? 0.0f : (pl == 1 ? 0.25f : (pl == 2 ? 0.5f : 0.25f));
-      if (pl < 3) {
-        sg[0][0] += w0 * px; sg[0][1] += w0 * py; sg[0][2] += w0 * pz;
-      }
-      if (pl > 0) {
-        sg[1][0] += w1 * px; sg[1][1] += w1 * py; sg[1][2] += w1 * pz;
-      }
+  if (a.has_ibm) {
+    const int cnt = a.tiles.count[T];
+    const int first_id = tid < a.tiles.cap ? a.tiles.list[(long long)T * a.tiles.cap + tid] : 0;  // speculative
+    const unsigned fbits = a.tiles.fmax[(a.t + 1) & 1];
+    __syncthreads();  // every thread has read the count
+    // Consumed: the particle pass of this step refills the list and records
+    // its force maximum in the other slot, cleared here.
+    if (tid == 0) {
+      a.tiles.count[T] = 0;
+      if (T == 0) a.tiles.fmax[a.t & 1] = 0u;
+    }
+    if (cnt > 0) {
+      accumulate_tile(sm, g, a.tiles, T, min(cnt, a.tiles.cap), X0, Y0, Z0, tid, fixed_exponent(fbits), first_id,
+                      a.err);
+      smooth_pair(sm, threadIdx.x, threadIdx.y, threadIdx.z, sg);
     }
   }
+
   int nclamp = 0;
 #pragma unroll 1
   for (int zz = 0; zz < 2; zz++) {
     const int z = Z0 + 2 * threadIdx.z + zz;
-    if (x < 1 || x > g.Nx - 2 || y < 1 || y > g.Ny - 2 || z < 1 || z > g.Nz - 2) continue;
+    if (!inxy || z < 1 || z > g.Nz - 2) continue;
     const int i = x + g.Nx * (y + g.Ny * z);
     float f[19];
-    if (FIRST) {
+    if (first) {
 #pragma unroll
       for (int q = 0; q < 19; q++) f[q] = Stored<ST>::load(fin + q * NC + i, WQ(q));
+    } else if (BC == BC_ZWALL) {
+      const int Nxy = g.Nx * g.Ny;
+      const int dxm = x == 1 ? g.Nx - 3 : -1;
+      const int dxp = x == g.Nx - 2 ? -(g.Nx - 3) : 1;
+      const int dym = (y == 1 ? g.Ny - 3 : -1) * g.Nx;
+      const int dyp = (y == g.Ny - 2 ? -(g.Ny - 3) : 1) * g.Nx;
+      gather(f, fin, NC, i, dxm, dxp, dym, dyp, -Nxy, Nxy);
+      if (z == 1) velocity_bc<2, 0>(f, a.p.velLower);
+      else if (z == g.Nz - 2) velocity_bc<2, 1>(f, a.p.velUpper);
     } else {
       int dxm, dxp, dym, dyp, dzm, dzp;
       neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
@@ -608,17 +686,17 @@ __global__ void __launch_bounds__(FLUID_THREADS, 4) fluid_step_kernel(const Flui
     // A non-finite population makes rho non-finite; a vanishing or negative
     // density is flagged too.
     if (!(rho > 0.0f && rho < 1e30f)) atomicOr(a.err, ERR_NONFINITE);
-    float tau = VAR ? a.tau[i] : a.p.tauN;
+    float tau = VISC != 0 ? a.tau[i] : a.p.tauN;
     bool clamped = false;
-    collide<COLL, VAR>(f, rho, ir, ux, uy, uz, gx, gy, gz, tau, a.p, clamped);
-    if (VAR) {
+    collide<COLL, VISC>(f, rho, ir, ux, uy, uz, gx, gy, gz, tau, a.p, clamped);
+    if (VISC != 0) {
       a.tau[i] = tau;
       nclamp += clamped ? 1 : 0;
     }
 #pragma unroll
     for (int q = 0; q < 19; q++) Stored<ST>::store(fout + q * NC + i, f[q], WQ(q));
   }
-  if (VAR && nclamp) atomicAdd(a.clamps, (unsigned long long)nclamp);
+  if (VISC != 0 && nclamp) atomicAdd(a.clamps, (unsigned long long)nclamp);
 }
 
 // Post-streaming, post-boundary populations of the last step (what the
@@ -646,7 +724,7 @@ __global__ void materialize_f_kernel(const FluidArgs a, float* __restrict__ out)
 
 // Dense spread-force field (the reference's gpf slot 0) from the tile lists,
 // for parity read-back.  One block per tile; does not consume the lists.
-__global__ void __launch_bounds__(256) spread_field_kernel(const Geom g, const TileLists tl, int last_step,
+__global__ void __launch_bounds__(FLUID_THREADS) spread_field_kernel(const Geom g, const TileLists tl, int last_step,
                                                            float* __restrict__ out, unsigned* err) {
   __shared__ SpreadSmem sm;
   const int tid = threadIdx.x;
@@ -654,8 +732,9 @@ __global__ void __launch_bounds__(256) spread_field_kernel(const Geom g, const T
   const int X0 = blockIdx.x * TILE_X, Y0 = blockIdx.y * TILE_Y, Z0 = blockIdx.z * TILE_Z;
   const int cnt = tl.count[T];
   if (cnt <= 0) return;
-  accumulate_tile(sm, g, tl, T, min(cnt, tl.cap), X0, Y0, Z0, tid, blockDim.x,
-                  fixed_exponent(tl.fmax[last_step & 1]), err);
+  const int first_id = tid < min(cnt, tl.cap) ? tl.list[T * tl.cap + tid] : 0;
+  accumulate_tile(sm, g, tl, T, min(cnt, tl.cap), X0, Y0, Z0, tid, fixed_exponent(tl.fmax[last_step & 1]), first_id,
+                  err);
   for (int k = tid; k < TILE_X * TILE_Y * TILE_Z; k += blockDim.x) {
     const int x = X0 + k % TILE_X, y = Y0 + (k / TILE_X) % TILE_Y, z = Z0 + k / (TILE_X * TILE_Y);
     if (x < 1 || x > g.Nx - 2 || y < 1 || y > g.Ny - 2 || z < 1 || z > g.Nz - 2) continue;
@@ -824,19 +903,26 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
   if ((int)blockIdx.x < ngroups) {
     const int grp = blockIdx.x;
     const int p = grp / nfa;
-    const Kin k = rigid_update(a, p);
-    if (grp % nfa == 0 && l == 0) {
-      a.kin_new[p] = k.x;
-      a.kin_new[p + np] = k.v;
-      a.kin_new[p + 2 * np] = k.q;
-      a.kin_new[p + 3 * np] = k.w;
+    const int wg = grp - p * nfa;  // work-group of the sphere
+    // The rigid-body update of the sphere, once per block and shared.
+    __shared__ Kin s_kin;
+    const float4 r0 = l < L ? a.sphere[wg * L + l] : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (l == 0) {
+      const Kin kn = rigid_update(a, p);
+      s_kin = kn;
+      if (wg == 0) {
+        a.kin_new[p] = kn.x;
+        a.kin_new[p + np] = kn.v;
+        a.kin_new[p + 2 * np] = kn.q;
+        a.kin_new[p + 3 * np] = kn.w;
+      }
     }
+    __syncthreads();
+    const Kin k = s_kin;
     float4 force = make_float4(0.f, 0.f, 0.f, 0.f), torque = force;
     int tx[4], ty[4], tz[4], nx = 0, ny = 0, nz = 0;
-    long long gid = (long long)grp * L + l;
+    const long long gid = (long long)grp * L + l;
     if (l < L) {
-      const int pt = (int)(gid % P.P);
-      const float4 r0 = a.sphere[pt];
       const float4 W = make_float4(P.S[0], P.S[1], P.S[2], 1.0f);
       const float4 rw = f4add(f4add(k.x, r0), W);
       const float4 rpp = make_float4(wrap_mod(rw.x, W.x), wrap_mod(rw.y, W.y), wrap_mod(rw.z, W.z), wrap_mod(rw.w, W.w));
@@ -879,41 +965,54 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
       }
     }
     // List the marker in every fluid tile whose halo holds one of its
-    // stencil nodes; lanes inserting into the same tile share one atomic.
-    // All atomics of the warp are issued before any result is used, so
+    // stencil nodes (up to 2 tiles per axis, 3 where the stencil wraps a
+    // periodic edge); lanes inserting into the same tile share one atomic.
+    // Up to 8 atomics of the warp are issued before any result is used, so
     // their round trips overlap.
     {
       const int n = nx * ny * nz;
       int nmax = n;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
-      int tileOf[8], baseOf[8];
-      unsigned peersOf[8];
+      // Entry j of the marker's tile product, j = ia + nx*(ib + ny*ic),
+      // advanced incrementally (no divisions).
+      int ia = 0, ib = 0, ic = 0;
+      for (int j0 = 0; j0 < nmax; j0 += 8) {
+        int tileOf[8], baseOf[8];
+        unsigned peersOf[8];
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        tileOf[j] = -1;
-        baseOf[j] = 0;
-        peersOf[j] = 0u;
-        if (j >= nmax) continue;
-        const bool act = j < n;
-        const unsigned amask = __ballot_sync(0xffffffffu, act);
-        if (act) {
-          const int ia = j % nx, ib = (j / nx) % ny, ic = j / (nx * ny);
-          const int T = tx[ia] + g.ntx * (ty[ib] + g.nty * tz[ic]);
-          const unsigned peers = __match_any_sync(amask, T);
-          tileOf[j] = T;
-          peersOf[j] = peers;
-          if (lane == __ffs(peers) - 1) baseOf[j] = atomicAdd(&a.tiles.count[T], __popc(peers));
+        for (int jj = 0; jj < 8; jj++) {
+          const int j = j0 + jj;
+          tileOf[jj] = -1;
+          baseOf[jj] = 0;
+          peersOf[jj] = 0u;
+          if (j >= nmax) continue;
+          const bool act = j < n;
+          const unsigned amask = __ballot_sync(0xffffffffu, act);
+          if (act) {
+            const int T = tx[ia] + g.ntx * (ty[ib] + g.nty * tz[ic]);
+            const unsigned peers = __match_any_sync(amask, T);
+            tileOf[jj] = T;
+            peersOf[jj] = peers;
+            if (lane == __ffs(peers) - 1) baseOf[jj] = atomicAdd(&a.tiles.count[T], __popc(peers));
+            if (++ia == nx) {
+              ia = 0;
+              if (++ib == ny) {
+                ib = 0;
+                ++ic;
+              }
+            }
+          }
         }
-      }
 #pragma unroll
-      for (int j = 0; j < 8; j++) {
-        if (j >= nmax) continue;
-        const int base = __shfl_sync(0xffffffffu, baseOf[j], peersOf[j] ? __ffs(peersOf[j]) - 1 : lane);
-        if (tileOf[j] >= 0) {
-          const int slot = base + __popc(peersOf[j] & ((1u << lane) - 1u));
-          if (slot < a.tiles.cap) a.tiles.list[(long long)tileOf[j] * a.tiles.cap + slot] = (int)gid;
-          else atomicOr(a.err, ERR_TILE_OVERFLOW);
+        for (int jj = 0; jj < 8; jj++) {
+          if (j0 + jj >= nmax) continue;
+          const int base = __shfl_sync(0xffffffffu, baseOf[jj], peersOf[jj] ? __ffs(peersOf[jj]) - 1 : lane);
+          if (tileOf[jj] >= 0) {
+            const int slot = base + __popc(peersOf[jj] & ((1u << lane) - 1u));
+            if (slot < a.tiles.cap) a.tiles.list[(long long)tileOf[jj] * a.tiles.cap + slot] = (int)gid;
+            else atomicOr(a.err, ERR_TILE_OVERFLOW);
+          }
         }
       }
     }
@@ -1117,22 +1216,35 @@ __global__ void load_f_kernel(const ST* __restrict__ in, float* __restrict__ out
 
 // ---------------------------------------------------------------------------
 // Launchers.
-template <bool FIRST, bool VAR, int COLL, typename ST>
-static cudaError_t launch_fluid_t(const FluidArgs& a, cudaStream_t s) {
+template <int COLL, int VISC, int BC, typename ST>
+static cudaError_t launch_fluid_t(const FluidArgs& a, bool first, cudaStream_t s) {
   dim3 block(TILE_X, TILE_Y, 2);
   dim3 grid(a.g.ntx, a.g.nty, a.g.ntz);
-  fluid_step_kernel<FIRST, VAR, COLL, ST><<<grid, block, 0, s>>>(a);
+  const size_t smem = fluid_smem_bytes(a.has_ibm != 0);
+  fluid_step_kernel<COLL, VISC, BC, ST><<<grid, block, smem, s>>>(a, first ? 1 : 0);
   return cudaGetLastError();
+}
+
+template <int COLL, int BC, typename ST>
+static cudaError_t launch_fluid_v(const FluidArgs& a, bool first, bool variable, cudaStream_t s) {
+  if (!variable) return launch_fluid_t<COLL, 0, BC, ST>(a, first, s);
+  switch (a.p.viscModel) {
+    case 2: return launch_fluid_t<COLL, 2, BC, ST>(a, first, s);
+    case 3: return launch_fluid_t<COLL, 3, BC, ST>(a, first, s);
+    case 4: return launch_fluid_t<COLL, 4, BC, ST>(a, first, s);
+    default: return launch_fluid_t<COLL, 1, BC, ST>(a, first, s);  // tau = NewtonianTau, stored
+  }
 }
 
 template <typename ST>
 static cudaError_t launch_fluid_st(const FluidArgs& a, bool first, bool variable, int collision, cudaStream_t s) {
-  if (collision == 0) {
-    if (first) return variable ? launch_fluid_t<true, true, 0, ST>(a, s) : launch_fluid_t<true, false, 0, ST>(a, s);
-    return variable ? launch_fluid_t<false, true, 0, ST>(a, s) : launch_fluid_t<false, false, 0, ST>(a, s);
-  }
-  if (first) return variable ? launch_fluid_t<true, true, 1, ST>(a, s) : launch_fluid_t<true, false, 1, ST>(a, s);
-  return variable ? launch_fluid_t<false, true, 1, ST>(a, s) : launch_fluid_t<false, false, 1, ST>(a, s);
+  const Geom& g = a.g;
+  const bool zwall = g.periodic[0] && g.periodic[1] && g.wallAxis == 2 && !g.tanBC[0] && !g.tanBC[1] && !g.tanBC[2];
+  if (collision == 0)
+    return zwall ? launch_fluid_v<0, BC_ZWALL, ST>(a, first, variable, s)
+                 : launch_fluid_v<0, BC_GENERIC, ST>(a, first, variable, s);
+  return zwall ? launch_fluid_v<1, BC_ZWALL, ST>(a, first, variable, s)
+               : launch_fluid_v<1, BC_GENERIC, ST>(a, first, variable, s);
 }
 
 cudaError_t launch_fluid(const FluidArgs& a, bool first, bool variable, int collision, int storage, cudaStream_t s) {
@@ -1169,8 +1281,10 @@ cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s) {
   const int threads = a.p.L < 128 ? 128 : a.p.L;
   const size_t smem = sizeof(float4) * 2 * threads;
   particle_step_kernel<<<ngroups, threads, smem, s>>>(a);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_contacts(const ParticleArgs& a, cudaStream_t s) {
   contact_kernel<<<(a.p.np + 3) / 4, 128, 0, s>>>(a);
   return cudaGetLastError();
 }
@@ -1183,7 +1297,7 @@ cudaError_t launch_zones(const ZoneArgs& a, cudaStream_t s) {
 cudaError_t launch_spread_field(const Geom& g, const TileLists& t, int last_step, float* out, unsigned* err,
                                 cudaStream_t s) {
   dim3 grid(g.ntx, g.nty, g.ntz);
-  spread_field_kernel<<<grid, 256, 0, s>>>(g, t, last_step, out, err);
+  spread_field_kernel<<<grid, FLUID_THREADS, 0, s>>>(g, t, last_step, out, err);
   return cudaGetLastError();
 }
 
