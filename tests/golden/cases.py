@@ -33,6 +33,16 @@ CASES = {
                         particle_diameter=6.0, initial_particle_distribution=3, initial_particle_buffer=0.5,
                         z_wall_particle_buffer=2.0, domain_decomposition=(1, 1, 1), rebuild_neigh_list_freq=5,
                         video_freq=6, fluid_ouput_spacing=3),
+    # A sphere (d=6) at the corner (0.5, 0.5, 0.5) of a fully periodic box
+    # whose N-2 is a multiple of the fluid tile in every axis (32, 16, 16):
+    # markers that wrap touch up to 2 x 3 x 3 = 18 tiles.  The sphere is 100
+    # times denser than the fluid, so it lags the body-force driven flow and
+    # its marker forces are well above rounding level.
+    "wrap_tile_edge": dict(COMMON, iterations=8, total_lattice_size=(34, 18, 18), boundary_conditions_xyz=(0, 0, 0),
+                           newtonian_tau=0.8, viscosity_model=1, constant_body_force=(1e-4, 0.0, 0.0),
+                           initial_vel=(0.01, 0.0, 0.0), num_particles=1, particle_diameter=6.0, particle_density=100.0,
+                           initial_particle_distribution=1, initial_particle_buffer=0.5, z_wall_particle_buffer=0.0,
+                           domain_decomposition=(1, 1, 1), rebuild_neigh_list_freq=5),
     # Eight overlapping spheres on a grid (harmonic contact + z-wall forces),
     # two particle threads, zone rebuilds every 4 steps.
     "contacts": dict(COMMON, iterations=12, total_lattice_size=(28, 28, 30), boundary_conditions_xyz=(0, 0, 1),

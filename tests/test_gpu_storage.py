@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 # Relative L2 of u after N steps: (Newtonian, non-Newtonian) per storage.
 U_TOL = {1: (1e-3, 1e-2), 2: (1e-2, 3e-2)}
 # Sphere velocities, force and torque partials in units of the problem's
-# scale (wall speed, summed marker force at that slip).
+# scale (wall speed or peak flow speed, summed marker force at that slip).
 PARTICLE_TOL = {1: 1e-4, 2: 1e-3}
 
 
@@ -49,7 +49,9 @@ def test_shifted_storage_against_reference(name, storage):
         assert rel_l2(sim.read_f()[mf], g["final_f"][mf]) <= tol
     if ip.NumParticles > 0:
         np_ = ip.NumParticles
-        U = max(abs(v) for v in list(fp.VelUpper) + list(fp.VelLower) + [1e-3])
+        # Velocity scale of the problem: the wall speeds, or the largest
+        # velocity of the reference's flow where no wall drives it.
+        U = max([abs(v) for v in list(fp.VelUpper) + list(fp.VelLower)] + [float(np.abs(g["final_u"][mu]).max()), 1e-3])
         R = fp.ParticleDiam / 2
         Fs = fp.PointArea * ip.PointsPerParticle * U / ip.WorkGroupsPerParticle
         kin = sim.read_parkin().reshape(-1, 4)
