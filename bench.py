@@ -16,6 +16,7 @@ runs an independent replica: weak scaling, no collective on the data path).
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -371,6 +372,9 @@ def cpu_baseline(workload, sample_steps=8):
 
 
 def run_reference_arm(args):
+    if args.workload not in REFERENCE_KEYWORDS:
+        return {"impl": "reference", "unavailable": f"{args.workload}: the reference runs one lattice per process and "
+                                                    "has no pool or request loop"}
     b = cpu_baseline(args.workload, sample_steps=max(1, min(args.steps, 8)))
     kw = WORKLOADS[args.workload]
     N = kw["total_lattice_size"]
@@ -387,13 +391,158 @@ def run_reference_arm(args):
     return out
 
 
+# ---------------------------------------------------------------------------
+# The lattice pool: batched uneven boxes and the served sweep.
+def batch_requests(n=64, seed=4):
+    """64 independent boxes: edges from {32,48,64,96} per axis, 1-20 spheres
+    of radius 4-8, power-law n in [0.4, 1], wall speed in [0.01, 0.05]."""
+    import numpy as np
+
+    from d3q19_b200 import serving as sv
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        edge = tuple(int(rng.choice([32, 48, 64, 96])) for _ in range(3))
+        d = float(rng.uniform(8.0, 16.0))
+        # 1-20 spheres, at most what fills a quarter of the slab their
+        # centres may occupy (random sequential addition must place them).
+        slab = (edge[0] - 2) * (edge[1] - 2) * max(edge[2] - 2 - d - 4, 0.0)
+        nsph = min(int(rng.integers(1, 21)), int(0.25 * slab / (math.pi / 6 * d ** 3)))
+        req = sv.ShearRequest(rid=i, edge=edge, phi=0.0, model="power_law", wall_speed=float(rng.uniform(0.01, 0.05)),
+                              seed=int(rng.integers(1, 2 ** 31 - 1)), diameter=d, n_index=float(rng.uniform(0.4, 1.0)))
+        kw = sv.solve_keywords(req)
+        # Sphere count as drawn (not from a volume fraction); the slab must
+        # hold the spheres' centres.
+        kw.update(num_particles=nsph)
+        if nsph > 0:
+            kw.update(particle_diameter=d, initial_particle_distribution=4, particle_seed=req.seed,
+                      min_particle_gap=0.0, initial_particle_buffer=0.0, z_wall_particle_buffer=d / 2 + 2,
+                      particle_collision_params=2.0)
+        out.append((req, kw))
+    return out
+
+
+def _time_pool(pool, steps, stream_ptr, torch):
+    stream = torch.cuda.ExternalStream(stream_ptr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    pool.advance(steps)
+    e1.record(stream)
+    pool.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_batch(args):
+    """cfg: 64 uneven boxes advanced together (FP16 shifted storage, chunks
+    of 1000 steps captured as graphs, grid sizes from the autotuner) against
+    the same boxes one at a time in FP32."""
+    import torch
+
+    import d3q19_b200 as d3
+
+    torch.cuda.set_device(0)
+    items = batch_requests()
+    states = [d3.HostState(d3.parse_config(d3.keywords_text(kw)), data_dir=os.getcwd()) for _, kw in items]
+    nodes = sum((hs.cfg.ip.LatticeSize[0] - 2) * (hs.cfg.ip.LatticeSize[1] - 2) * (hs.cfg.ip.LatticeSize[2] - 2)
+                for hs in states)
+    chunk = 1000
+    pool = d3.Pool(storage=1, max_slots=len(states), hbm_budget=120 << 30)
+    for hs in states:
+        if pool.admit(hs) is None:
+            raise RuntimeError("batch does not fit the pool")
+    # Autotuner: persistent grid sizes (CTAs per SM of the fluid, particle and
+    # contact passes), each timed on a 200-step chunk of the live batch (the
+    # results do not depend on the grid); the fastest is kept.
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    trials = []
+    for fb in (2, 3, 4):
+        for pb in (1, 2, 4):
+            pool.set_grid(fb * sms, pb * sms, pb * sms)
+            pool.advance(200)  # capture
+            trials.append((_time_pool(pool, 200, pool.stream_ptr, torch), fb, pb))
+    best = min(trials)
+    pool.set_grid(best[1] * sms, best[2] * sms, best[2] * sms)
+    pool.advance(chunk)  # capture of the 1000-step chunk
+    ms = _time_pool(pool, chunk * max(1, args.steps // chunk), pool.stream_ptr, torch)
+    steps = chunk * max(1, args.steps // chunk)
+    pool.close()
+    batched = nodes * steps / (ms * 1e-3) / 1e6
+    # One at a time, FP32, graph-replayed runs of the same step count each.
+    base_steps = 200
+    t_alone = 0.0
+    for hs in states:
+        sim = d3.Simulation.from_host_state(hs, device=0, storage=0)
+        sim.run(1, 64)
+        sim.synchronize()
+        stream = torch.cuda.ExternalStream(sim.stream_ptr)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.run(65, base_steps)
+        e1.record(stream)
+        sim.synchronize()
+        t_alone += e0.elapsed_time(e1)
+        sim.close()
+    alone = nodes * base_steps / (t_alone * 1e-3) / 1e6
+    return {"metric": "MLUPS (batched boxes)", "value": round(batched, 1), "unit": "MLUPS", "n_gpus": 1,
+            "steps": steps, "higher_is_better": True, "dtype": "f32 arithmetic, f16 shifted storage",
+            "data": "synthetic (seeded)", "impl": "ours",
+            "config": {"workload": "batch-64", "boxes": len(states), "interior_nodes": nodes,
+                       "description": "64 boxes, edges from {32,48,64,96} per axis, 1-20 spheres of radius 4-8, "
+                                      "power-law n in [0.4,1], walls +-[0.01,0.05]; one launch per pass for all"},
+            "autotune": {"fluid_ctas_per_sm": best[1], "particle_ctas_per_sm": best[2],
+                         "trials_ms_per_200_steps": [[round(t, 3), f, pp] for t, f, pp in trials]},
+            "one_at_a_time_fp32": {"value": round(alone, 1), "unit": "MLUPS"},
+            "speedup_vs_one_at_a_time_fp32": round(batched / alone, 2)}
+
+
+def run_served(args):
+    """cfg: Poisson arrivals (50/s, seeded) of shear-rheology solves, cubic
+    edge in [32, 64], volume fraction in [0, 0.3], Newtonian / power law /
+    Casson, each until the mean shear stress changes < 1e-4 relative over 500
+    steps (at most max_steps); FP16 pool with continuous batching against
+    one-at-a-time FP32."""
+    import numpy as np
+    import torch
+
+    import d3q19_b200 as d3
+    from d3q19_b200 import serving as sv
+
+    torch.cuda.set_device(0)
+    reqs = sv.make_requests(args.requests, 50.0, 2024, edges=(32, 64))
+    max_steps = 40000
+    pool = d3.Pool(storage=1, max_slots=256, hbm_budget=100 << 30)
+    recs, wall = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=max_steps).run(reqs)
+    pool.close()
+    served = sv.summary(recs, wall)
+    base, bwall = sv.one_at_a_time(reqs, storage=0, check_every=500, rel_tol=1e-4, max_steps=max_steps)
+    alone = sv.summary(base, bwall)
+    by = {r.rid: r for r in base}
+    visc_err = [abs(r.eff_viscosity - by[r.rid].eff_viscosity) / max(abs(by[r.rid].eff_viscosity), 1e-30)
+                for r in recs]
+    return {"metric": "solves/s (served sweep)", "value": round(served["solves_per_s"], 3), "unit": "solves/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f32 arithmetic, f16 shifted storage",
+            "data": "synthetic (seeded Poisson arrivals)", "impl": "ours",
+            "config": {"workload": "served-sweep", "requests": len(reqs), "arrival_rate_per_s": 50.0,
+                       "edges": [32, 64], "phi": [0.0, 0.3], "models": list(sv.MODELS), "stop": "1e-4 over 500 steps",
+                       "max_steps": max_steps},
+            "served": served, "one_at_a_time_fp32": alone,
+            "speedup_solves_per_s": round(served["solves_per_s"] / alone["solves_per_s"], 2),
+            "per_request": [[r.rid, r.steps, by[r.rid].steps, round(r.latency, 3), round(by[r.rid].latency, 3)]
+                            for r in sorted(recs, key=lambda r: r.rid)],
+            "eff_viscosity_rel_diff_fp16_pool_vs_fp32_alone": {"max": float(np.max(visc_err)),
+                                                               "median": float(np.median(visc_err))}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="dense-powerlaw-128", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="dense-powerlaw-128", choices=sorted(WORKLOADS) + ["batch-64",
+                                                                                           "served-sweep"])
+    ap.add_argument("--requests", type=int, default=128, help="served-sweep: number of requests")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", default="fp32", choices=sorted(STORAGE),
                     help="distribution storage: fp32 (the reference's), or 16-bit shifted")
@@ -406,6 +555,10 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference_arm(args)), flush=True)
+        return
+    if args.workload in ("batch-64", "served-sweep"):
+        if rank == 0:
+            print(json.dumps(run_batch(args) if args.workload == "batch-64" else run_served(args)), flush=True)
         return
     dist = None
     if world > 1:

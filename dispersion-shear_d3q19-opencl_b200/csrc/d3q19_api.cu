@@ -63,6 +63,7 @@ struct d3q19_ctx {
   int nzones = 0;
   unsigned* err = nullptr;
   unsigned long long* clamps = nullptr;
+  double* pstats = nullptr;  // per-plane FP64 sums [5 * Nz]
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
   bool have_particles = false, have_zones = false;
@@ -229,6 +230,7 @@ extern "C" int d3q19_create(const int_param_struct* ip, const flp_param_struct* 
   p.tauMax = o.tau_max;
   p.tauMin = o.tau_min;
   p.cassonReg = o.casson_reg;
+  p.variable = o.variable_viscosity ? 1 : 0;
 
   ParticleParams& pp = c->ppar;
   memset(&pp, 0, sizeof(pp));
@@ -260,7 +262,8 @@ extern "C" int d3q19_create(const int_param_struct* ip, const flp_param_struct* 
   const size_t fbytes = (size_t)storage_bytes(o.storage) * 19 * NC;
   if ((rc = dalloc(c, (char**)&c->f[0], fbytes)) || (rc = dalloc(c, (char**)&c->f[1], fbytes)) ||
       (rc = dalloc(c, &c->u, 3 * NC)) ||
-      (rc = dalloc(c, &c->tau, NC)) || (rc = dalloc(c, &c->err, 1)) || (rc = dalloc(c, &c->clamps, 1))) {
+      (rc = dalloc(c, &c->tau, NC)) || (rc = dalloc(c, &c->err, 1)) || (rc = dalloc(c, &c->clamps, 1)) ||
+      (rc = dalloc(c, &c->pstats, 5LL * g.Nz))) {
     snprintf(g_create_error, sizeof(g_create_error), "%s", c->msg);
     d3q19_destroy(c);
     return rc;
@@ -485,13 +488,16 @@ static int check_ready(d3q19_ctx* c) {
   return 0;
 }
 
-static int enqueue_step(d3q19_ctx* c, int t) {
+// Kernel arguments of step t with buffer parities cur (distributions) and
+// pcur (particle state).
+static FluidArgs fluid_args(const d3q19_ctx* c, int t, int cur) {
   FluidArgs fa;
+  memset(&fa, 0, sizeof(fa));
   fa.g = c->g;
   fa.p = c->fpar;
   fa.t = t;
-  fa.fin = c->f[c->cur];
-  fa.fout = c->f[1 - c->cur];
+  fa.fin = c->f[cur];
+  fa.fout = c->f[1 - cur];
   fa.u = c->u;
   fa.tau = c->tau;
   fa.tiles.cap = c->tile_cap;
@@ -502,6 +508,55 @@ static int enqueue_step(d3q19_ctx* c, int t) {
   fa.has_ibm = c->ppar.np > 0;
   fa.err = c->err;
   fa.clamps = c->clamps;
+  return fa;
+}
+
+static ParticleArgs particle_args(const d3q19_ctx* c, int t, int pcur) {
+  ParticleArgs pa;
+  memset(&pa, 0, sizeof(pa));
+  pa.g = c->g;
+  pa.p = c->ppar;
+  pa.kin_old = c->kin[pcur];
+  pa.kin_new = c->kin[1 - pcur];
+  pa.pff_old = c->pff[pcur];
+  pa.pff_new = c->pff[1 - pcur];
+  pa.pf_old = c->pf[pcur];
+  pa.pf_new = c->pf[1 - pcur];
+  pa.sphere = c->sphere;
+  pa.u = c->u;
+  pa.mrec = c->mrec;
+  pa.tiles.cap = c->tile_cap;
+  pa.tiles.count = c->tile_count;
+  pa.tiles.list = c->tile_list;
+  pa.tiles.mrec = c->mrec;
+  pa.tiles.fmax = c->fmax;
+  pa.znd = c->znd;
+  pa.parsZone = c->parsZone;
+  pa.zoneMembers = c->zoneMembers;
+  pa.numParInZone = c->numParInZone;
+  pa.revStart = c->revStart;
+  pa.revList = c->revList;
+  pa.err = c->err;
+  pa.t = t;
+  return pa;
+}
+
+// Zone rebuild from the particle state in kin[pnew].
+static ZoneArgs zone_args(const d3q19_ctx* c, int pnew) {
+  ZoneArgs za;
+  memset(&za, 0, sizeof(za));
+  za.p = c->ppar;
+  za.kin = c->kin[pnew];
+  za.parsZone = c->parsZone;
+  za.zoneMembers = c->zoneMembers;
+  za.numParInZone = c->numParInZone;
+  za.zoneOf = c->zoneOf;
+  za.err = c->err;
+  return za;
+}
+
+static int enqueue_step(d3q19_ctx* c, int t) {
+  const FluidArgs fa = fluid_args(c, t, c->cur);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (c->profiling) {
     CUDA_TRY(c, cudaEventCreate(&e0));
@@ -521,27 +576,7 @@ static int enqueue_step(d3q19_ctx* c, int t) {
   c->cur = 1 - c->cur;
   c->f_state = 2;
   if (c->ppar.np > 0) {
-    ParticleArgs pa;
-    pa.g = c->g;
-    pa.p = c->ppar;
-    pa.kin_old = c->kin[c->pcur];
-    pa.kin_new = c->kin[1 - c->pcur];
-    pa.pff_old = c->pff[c->pcur];
-    pa.pff_new = c->pff[1 - c->pcur];
-    pa.pf_old = c->pf[c->pcur];
-    pa.pf_new = c->pf[1 - c->pcur];
-    pa.sphere = c->sphere;
-    pa.u = c->u;
-    pa.mrec = c->mrec;
-    pa.tiles = fa.tiles;
-    pa.znd = c->znd;
-    pa.parsZone = c->parsZone;
-    pa.zoneMembers = c->zoneMembers;
-    pa.numParInZone = c->numParInZone;
-    pa.revStart = c->revStart;
-    pa.revList = c->revList;
-    pa.err = c->err;
-    pa.t = t;
+    const ParticleArgs pa = particle_args(c, t, c->pcur);
     // The rigid-body update reads the contact forces of step t-1.
     if (c->side_pending) CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
     if (c->profiling) {
@@ -561,17 +596,7 @@ static int enqueue_step(d3q19_ctx* c, int t) {
     CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev_fork, 0));
     CUDA_TRY(c, launch_contacts(pa, c->side));
     c->pcur = 1 - c->pcur;
-    if (t % c->opt.rebuild_freq == 0) {
-      ZoneArgs za;
-      za.p = c->ppar;
-      za.kin = c->kin[c->pcur];
-      za.parsZone = c->parsZone;
-      za.zoneMembers = c->zoneMembers;
-      za.numParInZone = c->numParInZone;
-      za.zoneOf = c->zoneOf;
-      za.err = c->err;
-      CUDA_TRY(c, launch_zones(za, c->side));
-    }
+    if (t % c->opt.rebuild_freq == 0) CUDA_TRY(c, launch_zones(zone_args(c, c->pcur), c->side));
     CUDA_TRY(c, cudaEventRecord(c->ev_join, c->side));
     c->side_pending = true;
   }
@@ -772,6 +797,67 @@ extern "C" int d3q19_read_zones(d3q19_ctx* c, int* parsZone, int* zoneMembers, i
   return 0;
 }
 
+// Per-plane FP64 sums (plane_stats_kernel) of the last step, read back.
+extern "C" int d3q19_plane_stats(d3q19_ctx* c, double* out) {
+  if (!c || !out) return D3Q19_EINVAL;
+  if (c->f_state == 0) return fail(c, D3Q19_ESTATE, "lattice not written");
+  cudaSetDevice(c->dev);
+  if (int rc = join_side(c)) return rc;
+  CUDA_TRY(c, launch_plane_stats(c->g, c->u, c->tau, c->fp.NewtonianTau, c->opt.variable_viscosity, c->pstats,
+                                 c->stream));
+  return readback(c, out, (const double*)c->pstats, 5 * (size_t)c->g.Nz);
+}
+
+extern "C" int d3q19_shear_profile(d3q19_ctx* c, double* u_mean, double* wall_rate, double* region_rate) {
+  if (!c) return D3Q19_EINVAL;
+  const int Nz = c->g.Nz;
+  std::vector<double> ps(5 * (size_t)Nz);
+  if (int rc = d3q19_plane_stats(c, ps.data())) return rc;
+  const double nxy = (double)(c->g.Nx - 2) * (c->g.Ny - 2);
+  auto ux = [&](int z) { return ps[5 * (size_t)z] / nxy; };
+  if (u_mean) {
+    for (int z = 0; z < Nz; z++)
+      for (int d = 0; d < 3; d++) u_mean[3 * z + d] = (z >= 1 && z <= Nz - 2) ? ps[5 * (size_t)z + d] / nxy : 0.0;
+  }
+  if (wall_rate) {
+    // compute_shear_stress (D3Q19-OpenCL.c:690-725): forward differences over
+    // dz = 4 ending on plane 1 + dz + 1 and on plane Nz - 3, summed and
+    // divided by twice the plane's node count.
+    const int dz = 4, zA = 1 + dz + 1, zB = Nz - 2 - 1;
+    double sum = 0.0;
+    if (zA >= 1 && zA <= Nz - 2 && zA - dz >= 0) sum += (ps[5 * (size_t)zA] - ps[5 * (size_t)(zA - dz)]) / dz;
+    if (zB != zA && zB >= 1 && zB <= Nz - 2 && zB - dz >= 0) sum += (ps[5 * (size_t)zB] - ps[5 * (size_t)(zB - dz)]) / dz;
+    *wall_rate = sum / (2.0 * nxy);
+  }
+  if (region_rate) {
+    // D3Q19-OpenCL.c:739-744: across the planes that spheres can reach.  The
+    // reference indexes its profile without a range check; planes outside
+    // the lattice give 0 here, planes 0 and Nz-1 have a zero mean.
+    const int ib = (int)(c->fp.ParticleZBuffer + 1E-8) + (int)(c->fp.ParticleDiam / 2);
+    const int zbL = 1 + ib, zbU = Nz - 2 - ib;
+    const bool ok = zbL >= 0 && zbL < Nz && zbU >= 0 && zbU < Nz && zbU != zbL;
+    *region_rate = ok ? (ux(zbU) - ux(zbL)) / (zbU - zbL) : 0.0;
+  }
+  return 0;
+}
+
+extern "C" int d3q19_mean_stress(d3q19_ctx* c, double* stress_xz, double* shear_rate, double* eff_viscosity) {
+  if (!c) return D3Q19_EINVAL;
+  const int Nz = c->g.Nz;
+  std::vector<double> ps(5 * (size_t)Nz);
+  if (int rc = d3q19_plane_stats(c, ps.data())) return rc;
+  double g = 0.0, t = 0.0;
+  for (int z = 1; z <= Nz - 2; z++) {
+    g += ps[5 * (size_t)z + 3];
+    t += ps[5 * (size_t)z + 4];
+  }
+  const double n = (double)(c->g.Nx - 2) * (c->g.Ny - 2) * (Nz - 2);
+  if (stress_xz) *stress_xz = t / n;
+  if (shear_rate) *shear_rate = g / n;
+  if (eff_viscosity) *eff_viscosity = g != 0.0 ? t / g : 0.0;
+  return 0;
+}
+
 extern "C" long long d3q19_tau_clamp_count(d3q19_ctx* c) {
   if (!c) return -1;
   unsigned long long v = 0;
@@ -838,7 +924,7 @@ extern "C" int d3q19_destroy(d3q19_ctx* c) {
   drop_events(c);
   void* ptrs[] = {c->f[0], c->f[1], c->u, c->tau, c->kin[0], c->kin[1], c->pff[0], c->pff[1], c->pf[0], c->pf[1],
                   c->sphere, c->mrec, c->tile_count, c->fmax, c->tile_list, c->znd, c->parsZone, c->zoneMembers,
-                  c->numParInZone, c->revStart, c->revList, c->zoneOf, c->err, c->clamps, c->scratch};
+                  c->numParInZone, c->revStart, c->revList, c->zoneOf, c->err, c->clamps, c->pstats, c->scratch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -923,4 +1009,394 @@ extern "C" int d3q19_read_spread_force_static(d3q19_ctx* c, float* gpf0) {
       CUDA_TRY(c, launch_spread_field(c->g, tl, c->last_t, field, c->err, c->stream));
   }
   return readback(c, gpf0, (const float*)field, 3 * NC);
+}
+
+/* ---------------------------------------------------------------------------
+ * Device memory of a context, and the lattice pool.
+ * ------------------------------------------------------------------------- */
+static size_t round_alloc(size_t b) { return (b + 511) / 512 * 512; }
+
+extern "C" int d3q19_context_bytes(const int_param_struct* ip, const d3q19_options* opt, size_t* out) {
+  if (!ip || !out) return D3Q19_EINVAL;
+  d3q19_options o;
+  memset(&o, 0, sizeof(o));
+  if (opt) o = *opt;
+  if (o.storage < 0 || o.storage > 2) return D3Q19_EINVAL;
+  const long long NC = (long long)ip->LatticeSize[0] * ip->LatticeSize[1] * ip->LatticeSize[2];
+  const long long ntiles = (long long)((ip->LatticeSize[0] + TILE_X - 1) / TILE_X) *
+                           ((ip->LatticeSize[1] + TILE_Y - 1) / TILE_Y) * ((ip->LatticeSize[2] + TILE_Z - 1) / TILE_Z);
+  size_t b = 2 * round_alloc((size_t)storage_bytes(o.storage) * 19 * NC) + round_alloc(12 * (size_t)NC) +
+             round_alloc(4 * (size_t)NC) + 3 * 512 + round_alloc(40 * (size_t)ip->LatticeSize[2]);
+  const long long np = ip->NumParticles;
+  if (np > 0) {
+    const long long P = ip->PointsPerParticle, nfa = ip->WorkGroupsPerParticle, M = np * P;
+    const long long Z = (long long)ip->NumZones[0] * ip->NumZones[1] * ip->NumZones[2];
+    const long long cap = o.ibm_tile_capacity > 0 ? o.ibm_tile_capacity : std::min<long long>(M, 2048);
+    b += 2 * (round_alloc(64 * np) + round_alloc(32 * np * nfa) + round_alloc(32 * np));
+    b += round_alloc(16 * P) + round_alloc(32 * M) + round_alloc(4 * ntiles) + 512 + round_alloc(4 * ntiles * cap);
+    b += round_alloc(4 * 28 * Z) + round_alloc(4 * np) + round_alloc(4 * Z * np) + round_alloc(4 * Z) +
+         round_alloc(4 * (Z + 1)) + round_alloc(4 * 27 * Z) + round_alloc(4 * np);
+  }
+  *out = b;
+  return 0;
+}
+
+struct d3q19_pool {
+  int dev = 0;
+  int storage = 0;
+  int rebuild = 10;  // zone rebuild period shared by every member
+  int period = 10;   // lcm(2, rebuild): admissions and advances keep this phase
+  size_t budget = 0, used = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_done = nullptr;
+  std::vector<d3q19_ctx*> slot;  // nullptr: free
+  std::vector<size_t> slot_bytes;
+  std::vector<long long> slot_steps;
+  int max_slots = 0;
+  // Device copies of the per-slot kernel arguments (two buffer parities) and
+  // the packed work lists.
+  FluidArgs* d_fargs = nullptr;
+  ParticleArgs* d_pargs = nullptr;
+  ZoneArgs* d_zargs = nullptr;
+  int2* d_work = nullptr;  // three regions of work_cap items: fluid tiles, particle groups, contact spheres
+  int* d_zslots = nullptr;
+  int* d_counts = nullptr;  // [fluid, particle, contact, zone] item counts
+  size_t work_cap = 0;
+  long long nf = 0, ngr = 0, nsph = 0;  // item counts of the current lists
+  int part_threads = 128;
+  bool dirty = true;
+  int fblocks = 0, pblocks = 0, cblocks = 0;
+  std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  // (steps, fblocks, pblocks, cblocks)
+  long long steps = 0;
+  char msg[512] = {0};
+};
+
+static int pfail(d3q19_pool* p, int code, const char* fmt, ...) {
+  char* buf = p ? p->msg : g_create_error;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, 512, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define POOL_TRY(p, call)                                                                        \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) return pfail((p), D3Q19_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+static void pool_drop_graphs(d3q19_pool* p) {
+  for (auto& kv : p->graphs) cudaGraphExecDestroy(kv.second);
+  p->graphs.clear();
+}
+
+extern "C" int d3q19_pool_create(int device, int storage, int rebuild_freq, int max_slots, size_t hbm_budget,
+                                 d3q19_pool** out) {
+  if (!out || storage < 0 || storage > 2 || max_slots <= 0 || rebuild_freq <= 0)
+    return pfail(nullptr, D3Q19_EINVAL, "pool: invalid arguments");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return pfail(nullptr, D3Q19_ENODEV, "CUDA device %d not available", device);
+  cudaDeviceProp pr;
+  cudaGetDeviceProperties(&pr, device);
+  if (pr.major != 10) return pfail(nullptr, D3Q19_ENODEV, "device %s is sm_%d%d; this build is sm_100a", pr.name,
+                                   pr.major, pr.minor);
+  cudaSetDevice(device);
+  d3q19_pool* p = new d3q19_pool();
+  p->dev = device;
+  p->storage = storage;
+  p->rebuild = rebuild_freq;
+  p->period = 2 / gcd_i(2, rebuild_freq) * rebuild_freq;
+  p->max_slots = max_slots;
+  p->budget = hbm_budget;
+  p->slot.assign(max_slots, nullptr);
+  p->slot_bytes.assign(max_slots, 0);
+  p->slot_steps.assign(max_slots, 0);
+  // Persistent grids: blocks per SM the kernels' register and shared memory
+  // bounds allow (the autotuner may lower them).
+  p->fblocks = pr.multiProcessorCount * (storage == STORE_F32 ? 5 : 4);
+  p->pblocks = pr.multiProcessorCount * 4;
+  p->cblocks = pr.multiProcessorCount * 4;
+  if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->ev_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMalloc(&p->d_fargs, sizeof(FluidArgs) * 2 * max_slots) != cudaSuccess ||
+      cudaMalloc(&p->d_pargs, sizeof(ParticleArgs) * 2 * max_slots) != cudaSuccess ||
+      cudaMalloc(&p->d_zargs, sizeof(ZoneArgs) * 2 * max_slots) != cudaSuccess ||
+      cudaMalloc(&p->d_zslots, sizeof(int) * max_slots) != cudaSuccess ||
+      cudaMalloc(&p->d_counts, sizeof(int) * 4) != cudaSuccess) {
+    d3q19_pool_destroy(p);
+    return pfail(nullptr, D3Q19_ENOMEM, "pool: device set-up failed");
+  }
+  p->used = sizeof(FluidArgs) * 2 * max_slots + sizeof(ParticleArgs) * 2 * max_slots +
+            sizeof(ZoneArgs) * 2 * max_slots;
+  *out = p;
+  return 0;
+}
+
+extern "C" int d3q19_pool_admit(d3q19_pool* p, const int_param_struct* ip, const flp_param_struct* fp,
+                                const d3q19_options* opt, const float* f, const float* u, const float* tau,
+                                const float* parKin, const float* parForce, const float* parFluidForce,
+                                const float* spherePoints, const int* zoneNeighDat, const int* parsZone,
+                                const int* zoneMembers, const int* numParInZone, int* slot_out) {
+  if (!p || !ip || !fp || !f || !u || !slot_out) return D3Q19_EINVAL;
+  d3q19_options o;
+  memset(&o, 0, sizeof(o));
+  if (opt) o = *opt;
+  o.device = p->dev;
+  if (o.storage != p->storage) return pfail(p, D3Q19_EINVAL, "storage %d differs from the pool's %d", o.storage,
+                                            p->storage);
+  if (o.arithmetic != 0 || o.collision != 0)
+    return pfail(p, D3Q19_EINVAL, "the pool runs the fast arithmetic with the reference's MRT only");
+  if (ip->BoundaryConds[0] != 0 || ip->BoundaryConds[1] != 0 || ip->BoundaryConds[2] != 1 ||
+      o.tangential_vel_bc[0] || o.tangential_vel_bc[1] || o.tangential_vel_bc[2])
+    return pfail(p, D3Q19_EINVAL, "the pool runs shear cells: periodic x and y, velocity walls on z");
+  if (o.rebuild_freq <= 0) o.rebuild_freq = 10;
+  if (ip->NumParticles > 0 && o.rebuild_freq != p->rebuild)
+    return pfail(p, D3Q19_EINVAL, "rebuild_freq %d differs from the pool's %d", o.rebuild_freq, p->rebuild);
+  if (ip->NumParticles > 0 && ip->PointsPerWorkGroup > 256)
+    return pfail(p, D3Q19_EINVAL, "PointsPerWorkGroup above 256");
+  int s = -1;
+  for (int k = 0; k < p->max_slots && s < 0; k++)
+    if (!p->slot[k]) s = k;
+  if (s < 0) return pfail(p, D3Q19_EBUSY, "all %d slots are taken", p->max_slots);
+  size_t bytes = 0;
+  if (int rc = d3q19_context_bytes(ip, &o, &bytes)) return rc;
+  if (p->used + bytes > p->budget)
+    return pfail(p, D3Q19_EBUSY, "%zu bytes would exceed the HBM budget (%zu of %zu used)", bytes, p->used,
+                 p->budget);
+  d3q19_ctx* c = nullptr;
+  int rc = d3q19_create(ip, fp, &o, &c);
+  if (rc) return pfail(p, rc, "%s", d3q19_last_error(nullptr));
+  rc = d3q19_write_lattice(c, f, u, tau);
+  if (!rc && ip->NumParticles > 0) {
+    rc = d3q19_write_particles(c, parKin, parForce, parFluidForce, spherePoints);
+    if (!rc) rc = d3q19_write_zones(c, zoneNeighDat, parsZone, zoneMembers, numParInZone, nullptr, nullptr);
+  }
+  // The first steps run alone, so that the member joins in the pool's phase:
+  // its next step t satisfies t = 1 (mod period) like every other member's.
+  if (!rc) rc = d3q19_run(c, 1, p->period);
+  if (!rc) rc = d3q19_synchronize(c);
+  if (rc) {
+    pfail(p, rc, "admission: %s", d3q19_last_error(c));
+    d3q19_destroy(c);
+    return rc;
+  }
+  p->slot[s] = c;
+  p->slot_bytes[s] = bytes;
+  p->slot_steps[s] = p->period;
+  p->used += bytes;
+  p->dirty = true;
+  *slot_out = s;
+  return 0;
+}
+
+// Work lists and arguments of the members, uploaded on the pool's stream.
+static int pool_upload(d3q19_pool* p) {
+  std::vector<FluidArgs> fa(2 * (size_t)p->max_slots);
+  std::vector<ParticleArgs> pa(2 * (size_t)p->max_slots);
+  std::vector<ZoneArgs> za(2 * (size_t)p->max_slots);
+  std::vector<int2> fw, pw, cw;
+  std::vector<int> zs;
+  int threads = 128;
+  for (int s = 0; s < p->max_slots; s++) {
+    d3q19_ctx* c = p->slot[s];
+    if (!c) continue;
+    // Step j of a chunk (j = 0, 1, ...) runs with distributions parity
+    // cur + j and particle parity pcur + j; its step number has parity of
+    // j + 1 (only the parity enters the kernels).
+    for (int j = 0; j < 2; j++) {
+      fa[2 * s + j] = fluid_args(c, j + 1, (c->cur + j) & 1);
+      if (c->ppar.np > 0) {
+        pa[2 * s + j] = particle_args(c, j + 1, (c->pcur + j) & 1);
+        za[2 * s + j] = zone_args(c, (c->pcur + j + 1) & 1);
+      }
+    }
+    for (long long T = 0; T < c->ntiles; T++) fw.push_back(make_int2(s, (int)T));
+    if (c->ppar.np > 0) {
+      for (int gr = 0; gr < c->ppar.np * c->ppar.nfa; gr++) pw.push_back(make_int2(s, gr));
+      for (int q = 0; q < c->ppar.np; q++) cw.push_back(make_int2(s, q));
+      zs.push_back(s);
+      threads = std::max(threads, c->ppar.L);
+    }
+  }
+  // Each list has a fixed region, so captured launches stay valid while
+  // members come and go; only a larger allocation invalidates them.
+  const size_t need = std::max(fw.size(), std::max(pw.size(), cw.size()));
+  if (need > p->work_cap) {
+    POOL_TRY(p, cudaStreamSynchronize(p->stream));
+    const size_t cap = std::max<size_t>(need, 2 * p->work_cap) + 4096;
+    if (p->d_work) cudaFree(p->d_work);
+    p->d_work = nullptr;
+    p->work_cap = 0;
+    POOL_TRY(p, cudaMalloc(&p->d_work, sizeof(int2) * 3 * cap));
+    p->work_cap = cap;
+    pool_drop_graphs(p);  // the captured launches name the old list
+  }
+  p->nf = (long long)fw.size();
+  p->ngr = (long long)pw.size();
+  p->nsph = (long long)cw.size();
+  if (threads != p->part_threads) {
+    p->part_threads = threads;
+    pool_drop_graphs(p);
+  }
+  const int counts[4] = {(int)fw.size(), (int)pw.size(), (int)cw.size(), (int)zs.size()};
+  POOL_TRY(p, cudaMemcpyAsync(p->d_fargs, fa.data(), sizeof(FluidArgs) * fa.size(), cudaMemcpyHostToDevice,
+                              p->stream));
+  POOL_TRY(p, cudaMemcpyAsync(p->d_pargs, pa.data(), sizeof(ParticleArgs) * pa.size(), cudaMemcpyHostToDevice,
+                              p->stream));
+  POOL_TRY(p, cudaMemcpyAsync(p->d_zargs, za.data(), sizeof(ZoneArgs) * za.size(), cudaMemcpyHostToDevice,
+                              p->stream));
+  const std::vector<int2>* lists[3] = {&fw, &pw, &cw};
+  for (int k = 0; k < 3; k++)
+    if (!lists[k]->empty())
+      POOL_TRY(p, cudaMemcpyAsync(p->d_work + k * p->work_cap, lists[k]->data(), sizeof(int2) * lists[k]->size(),
+                                  cudaMemcpyHostToDevice, p->stream));
+  if (!zs.empty())
+    POOL_TRY(p, cudaMemcpyAsync(p->d_zslots, zs.data(), sizeof(int) * zs.size(), cudaMemcpyHostToDevice, p->stream));
+  POOL_TRY(p, cudaMemcpyAsync(p->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice, p->stream));
+  // The host vectors go out of scope: wait for the copies.
+  POOL_TRY(p, cudaStreamSynchronize(p->stream));
+  p->dirty = false;
+  return 0;
+}
+
+static int pool_enqueue(d3q19_pool* p, int nsteps) {
+  const int2* fw = p->d_work;
+  const int2* pw = p->d_work + p->work_cap;
+  const int2* cw = p->d_work + 2 * p->work_cap;
+  for (int j = 0; j < nsteps; j++) {
+    const int par = j & 1;
+    POOL_TRY(p, launch_fluid_batch(p->d_fargs, fw, p->d_counts + 0, par, p->storage, p->fblocks, p->stream));
+    POOL_TRY(p, launch_particle_batch(p->d_pargs, pw, p->d_counts + 1, par, p->part_threads, p->pblocks, p->stream));
+    POOL_TRY(p, launch_contact_batch(p->d_pargs, cw, p->d_counts + 2, par, p->cblocks, p->stream));
+    if ((j + 1) % p->rebuild == 0)
+      POOL_TRY(p, launch_zone_batch(p->d_zargs, p->d_zslots, p->d_counts + 3, par, p->max_slots, p->stream));
+  }
+  return 0;
+}
+
+extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
+  if (!p) return D3Q19_EINVAL;
+  if (nsteps <= 0 || nsteps % p->period != 0)
+    return pfail(p, D3Q19_EINVAL, "steps must be a positive multiple of %d", p->period);
+  cudaSetDevice(p->dev);
+  for (int s = 0; s < p->max_slots; s++)  // members' own streams (admission, read-backs) first
+    if (p->slot[s]) {
+      if (int rc = join_side(p->slot[s])) return pfail(p, rc, "%s", d3q19_last_error(p->slot[s]));
+      POOL_TRY(p, cudaEventRecord(p->slot[s]->ev_fork, p->slot[s]->stream));
+      POOL_TRY(p, cudaStreamWaitEvent(p->stream, p->slot[s]->ev_fork, 0));
+    }
+  if (p->dirty)
+    if (int rc = pool_upload(p)) return rc;
+  auto key = std::make_tuple(nsteps, p->fblocks, p->pblocks, p->cblocks);
+  auto it = p->graphs.find(key);
+  if (it == p->graphs.end()) {
+    cudaGraph_t graph;
+    POOL_TRY(p, cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = pool_enqueue(p, nsteps);
+    cudaError_t e = cudaStreamEndCapture(p->stream, &graph);
+    if (rc) return rc;
+    if (e != cudaSuccess) return pfail(p, D3Q19_ECUDA, "pool capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return pfail(p, D3Q19_ECUDA, "pool graph: %s", cudaGetErrorString(e));
+    it = p->graphs.emplace(key, exec).first;
+  }
+  POOL_TRY(p, cudaGraphLaunch(it->second, p->stream));
+  POOL_TRY(p, cudaEventRecord(p->ev_done, p->stream));
+  for (int s = 0; s < p->max_slots; s++) {
+    d3q19_ctx* c = p->slot[s];
+    if (!c) continue;
+    // nsteps is even: the buffer parities are where they were.
+    c->last_t += nsteps;
+    p->slot_steps[s] += nsteps;
+    POOL_TRY(p, cudaStreamWaitEvent(c->stream, p->ev_done, 0));  // read-backs after the pool's work
+  }
+  p->steps += nsteps;
+  return 0;
+}
+
+extern "C" d3q19_ctx* d3q19_pool_context(d3q19_pool* p, int slot) {
+  if (!p || slot < 0 || slot >= p->max_slots) return nullptr;
+  return p->slot[slot];
+}
+
+extern "C" long long d3q19_pool_slot_steps(d3q19_pool* p, int slot) {
+  if (!p || slot < 0 || slot >= p->max_slots || !p->slot[slot]) return -1;
+  return p->slot_steps[slot];
+}
+
+extern "C" int d3q19_pool_release(d3q19_pool* p, int slot) {
+  if (!p || slot < 0 || slot >= p->max_slots || !p->slot[slot]) return D3Q19_EINVAL;
+  cudaSetDevice(p->dev);
+  POOL_TRY(p, cudaStreamSynchronize(p->stream));
+  d3q19_destroy(p->slot[slot]);
+  p->slot[slot] = nullptr;
+  p->used -= p->slot_bytes[slot];
+  p->slot_bytes[slot] = 0;
+  p->slot_steps[slot] = 0;
+  p->dirty = true;
+  return 0;
+}
+
+extern "C" int d3q19_pool_usage(d3q19_pool* p, size_t* used, size_t* budget, int* members) {
+  if (!p) return D3Q19_EINVAL;
+  int n = 0;
+  for (auto* c : p->slot) n += c != nullptr;
+  if (used) *used = p->used;
+  if (budget) *budget = p->budget;
+  if (members) *members = n;
+  return 0;
+}
+
+extern "C" int d3q19_pool_set_grid(d3q19_pool* p, int fluid_blocks, int particle_blocks, int contact_blocks) {
+  if (!p || fluid_blocks <= 0 || particle_blocks <= 0 || contact_blocks <= 0) return D3Q19_EINVAL;
+  p->fblocks = fluid_blocks;
+  p->pblocks = particle_blocks;
+  p->cblocks = contact_blocks;
+  return 0;
+}
+
+extern "C" int d3q19_pool_get_grid(d3q19_pool* p, int* fluid_blocks, int* particle_blocks, int* contact_blocks) {
+  if (!p) return D3Q19_EINVAL;
+  if (fluid_blocks) *fluid_blocks = p->fblocks;
+  if (particle_blocks) *particle_blocks = p->pblocks;
+  if (contact_blocks) *contact_blocks = p->cblocks;
+  return 0;
+}
+
+extern "C" int d3q19_pool_synchronize(d3q19_pool* p) {
+  if (!p) return D3Q19_EINVAL;
+  cudaSetDevice(p->dev);
+  POOL_TRY(p, cudaStreamSynchronize(p->stream));
+  for (int s = 0; s < p->max_slots; s++)
+    if (p->slot[s])
+      if (int rc = d3q19_synchronize(p->slot[s]))
+        return pfail(p, rc, "member %d: %s", s, d3q19_last_error(p->slot[s]));
+  return 0;
+}
+
+extern "C" void* d3q19_pool_stream(d3q19_pool* p) { return p ? (void*)p->stream : nullptr; }
+
+extern "C" const char* d3q19_pool_last_error(d3q19_pool* p) { return p ? p->msg : g_create_error; }
+
+extern "C" int d3q19_pool_destroy(d3q19_pool* p) {
+  if (!p) return D3Q19_EINVAL;
+  cudaSetDevice(p->dev);
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  pool_drop_graphs(p);
+  for (auto*& c : p->slot)
+    if (c) {
+      d3q19_destroy(c);
+      c = nullptr;
+    }
+  void* ptrs[] = {p->d_fargs, p->d_pargs, p->d_zargs, p->d_work, p->d_zslots, p->d_counts};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (p->ev_done) cudaEventDestroy(p->ev_done);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+  return 0;
 }

@@ -53,6 +53,7 @@ struct FluidParams {
   float tauMax;         // 0 = no upper clamp
   float tauMin;         // lower clamp (the reference's MIN_TAU = 0.505)
   float cassonReg;      // 0 = none
+  int variable;         // local tau (read only by kernels that choose the law at run time)
 };
 
 // One IBM marker of the last particle pass, two float4 per marker:
@@ -150,9 +151,24 @@ cudaError_t launch_load_f(const void* in, float* out, long long NC, int storage,
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s);
 cudaError_t launch_contacts(const ParticleArgs& a, cudaStream_t s);
 cudaError_t launch_zones(const ZoneArgs& a, cudaStream_t s);
+// Batched passes over many lattices (the lattice pool): persistent grids of
+// `blocks` CTAs over packed work lists {slot, tile | group | sphere} whose
+// lengths are read on the device; per-lattice arguments slots[2*s + parity].
+cudaError_t launch_fluid_batch(const FluidArgs* slots, const int2* work, const int* nwork, int parity, int storage,
+                               int blocks, cudaStream_t s);
+cudaError_t launch_particle_batch(const ParticleArgs* slots, const int2* work, const int* nwork, int parity,
+                                  int threads, int blocks, cudaStream_t s);
+cudaError_t launch_contact_batch(const ParticleArgs* slots, const int2* work, const int* nwork, int parity,
+                                 int blocks, cudaStream_t s);
+cudaError_t launch_zone_batch(const ZoneArgs* args, const int* slots, const int* nslots, int parity, int max_slots,
+                              cudaStream_t s);
 cudaError_t launch_spread_field(const Geom& g, const TileLists& t, int last_step, float* out, unsigned* err,
                                 cudaStream_t s);
 cudaError_t launch_marker_cells(const float4* mrec, int M, int* cells, cudaStream_t s);
+// Per-plane FP64 sums of u, the shear rate du_x/dz + du_z/dx and the viscous
+// shear stress: out[5 * Nz].
+cudaError_t launch_plane_stats(const Geom& g, const float* u, const float* tau, float tauN, int variable,
+                               double* out, cudaStream_t s);
 // Reference-exact variants (d3q19_exact.cu, compiled without contraction).
 cudaError_t launch_fluid_exact(const FluidArgs& a, bool first, bool variable, int slots, cudaStream_t s);
 cudaError_t launch_spread_field_exact(const Geom& g, const TileLists& t, int slots, float* out, unsigned* err,

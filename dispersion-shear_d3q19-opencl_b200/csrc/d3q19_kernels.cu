@@ -272,7 +272,8 @@ __device__ __forceinline__ void boundaries(float (&f)[19], const Geom& g, const 
 // difference accumulate as a momentum drift.  COLL 0: the reference's rate
 // vector with 1/tau at rows 8,9,10,14,15 (GPU_program.cl:453, 567-568);
 // COLL 1: BGK.  VISC 0: constant tau; otherwise the local tau of viscosity
-// law VISC (1 Newtonian, 2 power law, 3 Herschel-Bulkley, 4 Casson).
+// law VISC (1 Newtonian, 2 power law, 3 Herschel-Bulkley, 4 Casson); -1:
+// both chosen at run time (p.variable, p.viscModel).
 template <int COLL, int VISC>
 __device__ __forceinline__ void collide(float (&f)[19], float rho, float ir, float ux, float uy, float uz, float gx,
                                         float gy, float gz, float& tau, const FluidParams& p, bool& clamped) {
@@ -357,7 +358,7 @@ __device__ __forceinline__ void collide(float (&f)[19], float rho, float ir, flo
     s1 = 1.19f; s2 = 1.40f; s4 = 1.20f; s6 = 1.20f; s11 = 1.20f; s12 = 1.40f; s13 = 1.40f; s16 = 1.98f;
   }
 
-  if (VISC != 0) {
+  if (VISC > 0 || (VISC < 0 && p.variable)) {
     // Strain rate from the relaxed non-equilibrium moments with tau(t-1)
     // (GPU_program.cl:459-562): the second moments of M^-1 S_old M d, which
     // only rows e, 3pxx, pww and the off-diagonal p carry.
@@ -607,16 +608,16 @@ __host__ __device__ constexpr size_t fluid_smem_bytes(bool ibm) { return ibm ? s
 // consecutive z-planes.  first != 0: the stored state is the reference's
 // post-stream buffer (after an upload), read in place without streaming.
 template <int COLL, int VISC, int BC, typename ST>
-__global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? FLUID_MIN_BLOCKS_F32 : FLUID_MIN_BLOCKS)
-    fluid_step_kernel(const FluidArgs a, const int first) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SpreadSmem& sm = *reinterpret_cast<SpreadSmem*>(smem_raw);
+__device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, const int bx, const int by,
+                                           const int bz, SpreadSmem& sm) {
   const ST* __restrict__ fin = static_cast<const ST*>(a.fin);
   ST* __restrict__ fout = static_cast<ST*>(a.fout);
   const Geom& g = a.g;
   const int tid = threadIdx.x + TILE_X * (threadIdx.y + TILE_Y * threadIdx.z);
-  const int X0 = blockIdx.x * TILE_X, Y0 = blockIdx.y * TILE_Y, Z0 = blockIdx.z * TILE_Z;
-  const int T = blockIdx.x + g.ntx * (blockIdx.y + g.nty * blockIdx.z);
+  const int X0 = bx * TILE_X, Y0 = by * TILE_Y, Z0 = bz * TILE_Z;
+  const int T = bx + g.ntx * (by + g.nty * bz);
+  constexpr bool kRuntimeVisc = VISC < 0;
+  const bool var = VISC > 0 || (kRuntimeVisc && a.p.variable);
   const int x = X0 + threadIdx.x;
   const int y = Y0 + threadIdx.y;
   const long long NC = g.NC;
@@ -686,17 +687,47 @@ __global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? FLUID_MIN_BLO
     // A non-finite population makes rho non-finite; a vanishing or negative
     // density is flagged too.
     if (!(rho > 0.0f && rho < 1e30f)) atomicOr(a.err, ERR_NONFINITE);
-    float tau = VISC != 0 ? a.tau[i] : a.p.tauN;
+    float tau = var ? a.tau[i] : a.p.tauN;
     bool clamped = false;
     collide<COLL, VISC>(f, rho, ir, ux, uy, uz, gx, gy, gz, tau, a.p, clamped);
-    if (VISC != 0) {
+    if (var) {
       a.tau[i] = tau;
       nclamp += clamped ? 1 : 0;
     }
 #pragma unroll
     for (int q = 0; q < 19; q++) Stored<ST>::store(fout + q * NC + i, f[q], WQ(q));
   }
-  if (VISC != 0 && nclamp) atomicAdd(a.clamps, (unsigned long long)nclamp);
+  if (var && nclamp) atomicAdd(a.clamps, (unsigned long long)nclamp);
+}
+
+template <int COLL, int VISC, int BC, typename ST>
+__global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? FLUID_MIN_BLOCKS_F32 : FLUID_MIN_BLOCKS)
+    fluid_step_kernel(const FluidArgs a, const int first) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fluid_tile<COLL, VISC, BC, ST>(a, first, blockIdx.x, blockIdx.y, blockIdx.z,
+                                 *reinterpret_cast<SpreadSmem*>(smem_raw));
+}
+
+// The collide-stream pass of many independent lattices in one persistent
+// launch: CTA b takes work items b, b + gridDim.x, ... of the packed list
+// work[k] = {slot, tile} (*nwork items).  slots[2*s + parity] holds lattice
+// s's arguments for steps of that buffer parity.  The reference's MRT rates,
+// periodic x/y with z walls, and each lattice's own viscosity law.
+template <typename ST>
+__global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? FLUID_MIN_BLOCKS_F32 : FLUID_MIN_BLOCKS)
+    fluid_batch_kernel(const FluidArgs* __restrict__ slots, const int2* __restrict__ work,
+                       const int* __restrict__ nwork, const int parity) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SpreadSmem& sm = *reinterpret_cast<SpreadSmem*>(smem_raw);
+  const int n = *nwork;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const int2 it = work[w];
+    const FluidArgs& a = slots[2 * it.x + parity];
+    const int ntx = a.g.ntx, nty = a.g.nty;
+    const int bx = it.y % ntx, by = (it.y / ntx) % nty, bz = it.y / (ntx * nty);
+    fluid_tile<0, -1, BC_ZWALL, ST>(a, 0, bx, by, bz, sm);
+    __syncthreads();  // the spread halo is reused by the next item
+  }
 }
 
 // Post-streaming, post-boundary populations of the last step (what the
@@ -891,21 +922,20 @@ __device__ bool pair_force(const ParticleParams& P, const Kin& A, const Kin& B, 
   return any;
 }
 
-// One block per reference work-group of markers (np*nfa blocks).
-__global__ void particle_step_kernel(const ParticleArgs a) {
-  extern __shared__ float4 red[];  // [2*blockDim.x]: forces, then torques
+// One reference work-group of markers (group grp of np*nfa) per block:
+// red holds 2*blockDim.x float4 (forces, then torques), s_kin the sphere's
+// updated state.
+__device__ __forceinline__ void particle_group(const ParticleArgs& a, const int grp, float4* red, Kin& s_kin) {
   const ParticleParams& P = a.p;
   const Geom& g = a.g;
   const int np = P.np, nfa = P.nfa, L = P.L;
   const int ngroups = np * nfa;
   const int l = threadIdx.x;
   const int lane = l & 31;
-  if ((int)blockIdx.x < ngroups) {
-    const int grp = blockIdx.x;
+  {
     const int p = grp / nfa;
     const int wg = grp - p * nfa;  // work-group of the sphere
     // The rigid-body update of the sphere, once per block and shared.
-    __shared__ Kin s_kin;
     const float4 r0 = l < L ? a.sphere[wg * L + l] : make_float4(0.f, 0.f, 0.f, 0.f);
     if (l == 0) {
       const Kin kn = rigid_update(a, p);
@@ -1042,26 +1072,40 @@ __global__ void particle_step_kernel(const ParticleArgs a) {
       a.pff_new[grp] = red[0];
       a.pff_new[grp + ngroups] = red[B];
     }
-    return;
   }
+}
 
+__global__ void particle_step_kernel(const ParticleArgs a) {
+  extern __shared__ float4 red[];
+  __shared__ Kin s_kin;
+  particle_group(a, blockIdx.x, red, s_kin);
+}
+
+// The particle pass of many lattices in one persistent launch: work items
+// {slot, group} of the packed list, arguments slots[2*s + parity].
+__global__ void particle_batch_kernel(const ParticleArgs* __restrict__ slots, const int2* __restrict__ work,
+                                      const int* __restrict__ nwork, const int parity) {
+  extern __shared__ float4 red[];
+  __shared__ Kin s_kin;
+  const int n = *nwork;
+  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    const int2 it = work[w];
+    particle_group(slots[2 * it.x + parity], it.y, red, s_kin);
+    __syncthreads();  // red and s_kin are reused by the next item
+  }
 }
 
 // Particle-particle forces (CPU_program.cl:76-184) from the positions the
 // particle pass of this step wrote, after it (the reference's order:
 // particle_dynamics, IBM, particle_particle_forces).  One warp per sphere pi.
-__global__ void contact_kernel(const ParticleArgs a) {
+__device__ __forceinline__ void contact_sphere(const ParticleArgs& a, const int pi, const int lane) {
   const ParticleParams& P = a.p;
   const int np = P.np;
-  const int l = threadIdx.x;
-  const int lane = l & 31;
   // Every pair occurrence the reference's zone loops produce for pi: as the
   // higher index (neighbour zones of pi's zone, members pj < pi; lane t takes
   // neighbour entry t) and as the lower one (zones whose neighbour list names
   // pi's zone, members pk > pi; lanes over the reverse table), then a fixed
   // shuffle reduction: deterministic.
-  const int pi = blockIdx.x * (blockDim.x / 32) + (l >> 5);
-  if (pi >= np) return;  // whole warps
   const int nzones = P.numZones[0] * P.numZones[1] * P.numZones[2];
   const Kin ki = load_kin(a.kin_new, pi, np);
   float4 F = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1156,11 +1200,29 @@ __global__ void contact_kernel(const ParticleArgs a) {
   a.pf_new[pi + np] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
+// One warp per sphere.
+__global__ void contact_kernel(const ParticleArgs a) {
+  const int pi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  if (pi >= a.p.np) return;  // whole warps
+  contact_sphere(a, pi, threadIdx.x & 31);
+}
+
+// Contacts of many lattices: one warp per work item {slot, sphere}.
+__global__ void contact_batch_kernel(const ParticleArgs* __restrict__ slots, const int2* __restrict__ work,
+                                     const int* __restrict__ nwork, const int parity) {
+  const int n = *nwork;
+  const int warps = gridDim.x * (blockDim.x / 32);
+  for (int w = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); w < n; w += warps) {
+    const int2 it = work[w];
+    contact_sphere(slots[2 * it.x + parity], it.y, threadIdx.x & 31);
+  }
+}
+
 
 // update_particle_zones (CPU_program.cl:280-315) for all spheres: members of
 // each zone listed in increasing sphere index, the order the reference's
 // serial work-item loop produces.
-__global__ void zone_rebuild_kernel(const ZoneArgs a) {
+__device__ __forceinline__ void zone_rebuild(const ZoneArgs& a) {
   const ParticleParams& P = a.p;
   const int np = P.np;
   const int nz = P.numZones[0] * P.numZones[1] * P.numZones[2];
@@ -1182,6 +1244,77 @@ __global__ void zone_rebuild_kernel(const ZoneArgs a) {
       if (a.zoneOf[p] == z) a.zoneMembers[z * np + c++] = p;
     a.numParInZone[z] = c;
   }
+}
+
+__global__ void zone_rebuild_kernel(const ZoneArgs a) { zone_rebuild(a); }
+
+// Zone rebuilds of many lattices: block b rebuilds lattice slots[b].
+__global__ void zone_batch_kernel(const ZoneArgs* __restrict__ args, const int* __restrict__ slots,
+                                  const int* __restrict__ nslots, const int parity) {
+  if ((int)blockIdx.x >= *nslots) return;
+  zone_rebuild(args[2 * slots[blockIdx.x] + parity]);
+}
+
+// Per-plane FP64 sums over the interior nodes of z-plane blockIdx.x:
+// out[5*z + 0..2] = sums of u_x, u_y, u_z, out[5*z + 3] = sum of the shear
+// rate g_xz = du_x/dz + du_z/dx, out[5*z + 4] = sum of the viscous shear
+// stress nu * g_xz with nu = (tau - 1/2)/3 (lattice units, rho = 1).
+// Derivatives are central, wrapped on periodic axes and one-sided on the
+// wall layers (the wet nodes at 1 and N-2).  The reduction order is fixed,
+// so the sums are deterministic.
+__device__ __forceinline__ int axis_step(int c, int d, int N, bool periodic) {
+  // Neighbour c+d along an axis of interior nodes 1..N-2: wrapped when
+  // periodic, clamped (one-sided difference) otherwise.
+  int n = c + d;
+  if (n < 1) n = periodic ? N - 2 : 1;
+  if (n > N - 2) n = periodic ? 1 : N - 2;
+  return n;
+}
+
+__global__ void __launch_bounds__(256) plane_stats_kernel(const Geom g, const float* __restrict__ u,
+                                                          const float* __restrict__ tau, float tauN, int variable,
+                                                          double* __restrict__ out) {
+  __shared__ double red[5][256];
+  const int z = blockIdx.x;
+  const int tid = threadIdx.x;
+  double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (z >= 1 && z <= g.Nz - 2) {
+    const long long NC = g.NC;
+    const int nx = g.Nx - 2, ny = g.Ny - 2;
+    const int zm = axis_step(z, -1, g.Nz, g.periodic[2]), zp = axis_step(z, 1, g.Nz, g.periodic[2]);
+    for (int k = tid; k < nx * ny; k += 256) {
+      const int x = 1 + k % nx, y = 1 + k / nx;
+      const long long i = x + (long long)g.Nx * (y + (long long)g.Ny * z);
+      const int xm = axis_step(x, -1, g.Nx, g.periodic[0]), xp = axis_step(x, 1, g.Nx, g.periodic[0]);
+      const long long row = (long long)g.Nx * (y + (long long)g.Ny * z);
+      const long long izm = x + (long long)g.Nx * (y + (long long)g.Ny * zm);
+      const long long izp = x + (long long)g.Nx * (y + (long long)g.Ny * zp);
+      const double ux = u[i], uy = u[i + NC], uz = u[i + 2 * NC];
+      // Spacing of the difference: 2 for a central one, 1 for a one-sided
+      // one, 0 for a single-node axis (no gradient).
+      const int hz = (zp != z) + (zm != z), hx = (xp != x) + (xm != x);
+      const double dudz = hz ? ((double)u[izp] - (double)u[izm]) / hz : 0.0;
+      const double dwdx = hx ? ((double)u[row + xp + 2 * NC] - (double)u[row + xm + 2 * NC]) / hx : 0.0;
+      const double gxz = dudz + dwdx;
+      const double nu = ((variable ? (double)tau[i] : (double)tauN) - 0.5) / 3.0;
+      s[0] += ux;
+      s[1] += uy;
+      s[2] += uz;
+      s[3] += gxz;
+      s[4] += nu * gxz;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 5; c++) red[c][tid] = s[c];
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (tid < w) {
+#pragma unroll
+      for (int c = 0; c < 5; c++) red[c][tid] += red[c][tid + w];
+    }
+    __syncthreads();
+  }
+  if (tid < 5) out[5 * z + tid] = red[tid][0];
 }
 
 __global__ void marker_cells_kernel(const float4* mrec, int M, int* cells) {
@@ -1289,6 +1422,37 @@ cudaError_t launch_contacts(const ParticleArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// Batched passes (the lattice pool): fixed persistent grids, the work list
+// lengths live on the device so one captured sequence serves any mix.
+cudaError_t launch_fluid_batch(const FluidArgs* slots, const int2* work, const int* nwork, int parity, int storage,
+                               int blocks, cudaStream_t s) {
+  const dim3 block(TILE_X, TILE_Y, 2);
+  const size_t smem = fluid_smem_bytes(true);
+  if (storage == STORE_F16) fluid_batch_kernel<__half><<<blocks, block, smem, s>>>(slots, work, nwork, parity);
+  else if (storage == STORE_BF16)
+    fluid_batch_kernel<__nv_bfloat16><<<blocks, block, smem, s>>>(slots, work, nwork, parity);
+  else fluid_batch_kernel<float><<<blocks, block, smem, s>>>(slots, work, nwork, parity);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_particle_batch(const ParticleArgs* slots, const int2* work, const int* nwork, int parity,
+                                  int threads, int blocks, cudaStream_t s) {
+  particle_batch_kernel<<<blocks, threads, sizeof(float4) * 2 * threads, s>>>(slots, work, nwork, parity);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_contact_batch(const ParticleArgs* slots, const int2* work, const int* nwork, int parity,
+                                 int blocks, cudaStream_t s) {
+  contact_batch_kernel<<<blocks, 128, 0, s>>>(slots, work, nwork, parity);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zone_batch(const ZoneArgs* args, const int* slots, const int* nslots, int parity, int max_slots,
+                              cudaStream_t s) {
+  zone_batch_kernel<<<max_slots, 1024, 0, s>>>(args, slots, nslots, parity);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_zones(const ZoneArgs& a, cudaStream_t s) {
   zone_rebuild_kernel<<<1, 1024, 0, s>>>(a);
   return cudaGetLastError();
@@ -1298,6 +1462,12 @@ cudaError_t launch_spread_field(const Geom& g, const TileLists& t, int last_step
                                 cudaStream_t s) {
   dim3 grid(g.ntx, g.nty, g.ntz);
   spread_field_kernel<<<grid, FLUID_THREADS, 0, s>>>(g, t, last_step, out, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plane_stats(const Geom& g, const float* u, const float* tau, float tauN, int variable,
+                               double* out, cudaStream_t s) {
+  plane_stats_kernel<<<g.Nz, 256, 0, s>>>(g, u, tau, tauN, variable, out);
   return cudaGetLastError();
 }
 

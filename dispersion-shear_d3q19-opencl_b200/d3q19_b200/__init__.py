@@ -7,6 +7,7 @@ usable sm_100 device) is missing, the calls raise -- there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -19,7 +20,8 @@ HOST_LIB = os.path.join(LIBDIR, "libd3q19_host.so")
 # Largest lattice (N_C nodes) d3q19_read_spread_force_static accepts.
 STATIC_SPREAD_MAX_CELLS = 262144
 STATUS = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ENODEV", -5: "EOVERFLOW", -6: "ENUMERIC",
-          -7: "ESTATE"}
+          -7: "ESTATE", -8: "EBUSY"}
+EBUSY = -8
 
 _INT_FIELDS = [
     ("MaxIterations", 1), ("BasisVel", 57), ("LatticeSize", 3), ("SystemSize", 3), ("BufferSize", 3),
@@ -106,7 +108,8 @@ def cuda_lib():
         for name in ("d3q19_write_lattice", "d3q19_write_particles", "d3q19_write_zones", "d3q19_read_u",
                      "d3q19_read_tau", "d3q19_read_parkin", "d3q19_read_parforce", "d3q19_read_parfluidforce",
                      "d3q19_read_f", "d3q19_read_spread_force", "d3q19_read_spread_force_static",
-                     "d3q19_read_marker_cells", "d3q19_read_zones",
+                     "d3q19_read_marker_cells", "d3q19_read_zones", "d3q19_plane_stats", "d3q19_shear_profile",
+                     "d3q19_mean_stress",
                      "d3q19_synchronize", "d3q19_destroy", "d3q19_write_periodic_map"):
             getattr(lib, name).restype = C.c_int
         lib.d3q19_step.argtypes = [P, C.c_int]
@@ -115,6 +118,25 @@ def cuda_lib():
                                            C.POINTER(C.c_int)]
         lib.d3q19_run.argtypes = [P, C.c_int, C.c_int]
         lib.d3q19_write_periodic_map.argtypes = [P, P, C.c_int]
+        lib.d3q19_context_bytes.argtypes = [C.POINTER(IntParams), C.POINTER(Options), C.POINTER(C.c_size_t)]
+        lib.d3q19_pool_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]
+        lib.d3q19_pool_admit.argtypes = [P, C.POINTER(IntParams), C.POINTER(FlpParams), C.POINTER(Options)] + \
+            [P] * 11 + [C.POINTER(C.c_int)]
+        lib.d3q19_pool_advance.argtypes = [P, C.c_int]
+        lib.d3q19_pool_context.restype = P
+        lib.d3q19_pool_context.argtypes = [P, C.c_int]
+        lib.d3q19_pool_slot_steps.restype = C.c_longlong
+        lib.d3q19_pool_slot_steps.argtypes = [P, C.c_int]
+        lib.d3q19_pool_release.argtypes = [P, C.c_int]
+        lib.d3q19_pool_usage.argtypes = [P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
+        lib.d3q19_pool_set_grid.argtypes = [P, C.c_int, C.c_int, C.c_int]
+        lib.d3q19_pool_get_grid.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        lib.d3q19_pool_synchronize.argtypes = [P]
+        lib.d3q19_pool_stream.restype = P
+        lib.d3q19_pool_stream.argtypes = [P]
+        lib.d3q19_pool_last_error.restype = C.c_char_p
+        lib.d3q19_pool_last_error.argtypes = [P]
+        lib.d3q19_pool_destroy.argtypes = [P]
         _cuda = lib
     return _cuda
 
@@ -341,6 +363,25 @@ class Simulation:
         self._check(self.lib.d3q19_read_zones(self.h, _ptr(pz), _ptr(zm), _ptr(nz)), "read_zones")
         return pz, zm, nz
 
+    def plane_stats(self):
+        """Per-plane FP64 sums, shape (Nz, 5): u_x, u_y, u_z, shear rate,
+        viscous shear stress (d3q19_plane_stats)."""
+        return self._read("d3q19_plane_stats", 5 * self.ip.LatticeSize[2], np.float64).reshape(-1, 5)
+
+    def shear_profile(self):
+        """(u_mean (Nz, 3), wall shear rate, particle-region shear rate), the
+        quantities of the reference's compute_shear_stress, in FP64."""
+        um = np.zeros(3 * self.ip.LatticeSize[2], np.float64)
+        w, r = C.c_double(), C.c_double()
+        self._check(self.lib.d3q19_shear_profile(self.h, _ptr(um), C.byref(w), C.byref(r)), "shear_profile")
+        return um.reshape(-1, 3), w.value, r.value
+
+    def mean_stress(self):
+        """(mean viscous shear stress, mean shear rate, effective viscosity)."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        self._check(self.lib.d3q19_mean_stress(self.h, C.byref(a), C.byref(b), C.byref(c)), "mean_stress")
+        return a.value, b.value, c.value
+
     def profile(self, enable: bool):
         self._check(self.lib.d3q19_profile(self.h, int(enable)), "profile")
 
@@ -359,9 +400,130 @@ class Simulation:
         return int(self.lib.d3q19_tau_clamp_count(self.h))
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and getattr(self, "owned", True):
             self.lib.d3q19_destroy(self.h)
+        self.h = None
+
+    @classmethod
+    def _view(cls, lib, handle, ip: IntParams, fp: FlpParams, options: Options):
+        """A context owned by someone else (a pool member): read-backs only."""
+        sim = cls.__new__(cls)
+        sim.lib, sim.h, sim.owned = lib, handle, False
+        sim.ip = IntParams.from_buffer_copy(bytes(ip))
+        sim.fp = FlpParams.from_buffer_copy(bytes(fp))
+        sim.options = options
+        sim.nc = sim.ip.LatticeSize[0] * sim.ip.LatticeSize[1] * sim.ip.LatticeSize[2]
+        sim.np = sim.ip.NumParticles
+        sim.nfa = max(sim.ip.WorkGroupsPerParticle, 1)
+        sim.nzones = sim.ip.NumZones[0] * sim.ip.NumZones[1] * sim.ip.NumZones[2]
+        return sim
+
+
+def context_bytes(ip: IntParams, options: Options | None = None) -> int:
+    """Device memory a context of these parameters allocates (host-side
+    arithmetic, no GPU needed)."""
+    out = C.c_size_t()
+    rc = cuda_lib().d3q19_context_bytes(C.byref(ip), C.byref(options or Options()), C.byref(out))
+    if rc:
+        raise D3Q19Error(f"d3q19_context_bytes: {STATUS.get(rc, rc)}")
+    return int(out.value)
+
+
+class Pool:
+    """Many independent shear cells resident on one GPU, advanced together in
+    batched persistent kernels (d3q19_pool_* of the C ABI)."""
+
+    def __init__(self, device: int = 0, storage: int = 0, rebuild_freq: int = 10, max_slots: int = 256,
+                 hbm_budget: int = 64 << 30):
+        self.lib = cuda_lib()
+        h = C.c_void_p()
+        rc = self.lib.d3q19_pool_create(device, storage, rebuild_freq, max_slots, hbm_budget, C.byref(h))
+        if rc:
+            raise D3Q19Error(f"d3q19_pool_create: {STATUS.get(rc, rc)}: {self.lib.d3q19_pool_last_error(None).decode()}")
+        self.h = h
+        self.storage = storage
+        self.rebuild_freq = rebuild_freq
+        self.period = 2 // math.gcd(2, rebuild_freq) * rebuild_freq
+        self.members = {}
+
+    def _check(self, rc, what):
+        if rc:
+            raise D3Q19Error(f"{what}: {STATUS.get(rc, rc)}: {self.lib.d3q19_pool_last_error(self.h).decode()}")
+
+    def admit(self, hs: "HostState", **option_overrides):
+        """Admits the solve of a HostState; returns its slot, or None when the
+        pool has no room for it now (EBUSY)."""
+        opt = Options.from_buffer_copy(bytes(hs.options))
+        opt.storage = self.storage
+        opt.rebuild_freq = self.rebuild_freq
+        for k, v in option_overrides.items():
+            setattr(opt, k, v)
+        slot = C.c_int(-1)
+        arrs = [np.ascontiguousarray(x, np.float32) for x in (hs.f, hs.u, hs.tau)]
+        if hs.cfg.ip.NumParticles > 0:
+            arrs += [np.ascontiguousarray(x, np.float32) for x in (hs.parKin, hs.parForce, hs.parFluidForce,
+                                                                  hs.spherePoints)]
+            arrs += [np.ascontiguousarray(x, np.int32) for x in (hs.zoneNeighDat, hs.parsZone, hs.zoneMembers,
+                                                                hs.numParInZone)]
+        else:
+            arrs += [None] * 8
+        rc = self.lib.d3q19_pool_admit(self.h, C.byref(hs.cfg.ip), C.byref(hs.cfg.fp), C.byref(opt),
+                                       *[_ptr(a) for a in arrs], C.byref(slot))
+        if rc == EBUSY:
+            return None
+        self._check(rc, "pool_admit")
+        self.members[slot.value] = (IntParams.from_buffer_copy(bytes(hs.cfg.ip)),
+                                    FlpParams.from_buffer_copy(bytes(hs.cfg.fp)), opt)
+        return slot.value
+
+    def advance(self, nsteps: int):
+        self._check(self.lib.d3q19_pool_advance(self.h, nsteps), "pool_advance")
+
+    def member(self, slot: int) -> Simulation:
+        """Read-back view of a member (not stepped directly)."""
+        hnd = self.lib.d3q19_pool_context(self.h, slot)
+        if not hnd:
+            raise D3Q19Error(f"pool slot {slot} is free")
+        ip, fp, opt = self.members[slot]
+        return Simulation._view(self.lib, C.c_void_p(hnd), ip, fp, opt)
+
+    def steps(self, slot: int) -> int:
+        return int(self.lib.d3q19_pool_slot_steps(self.h, slot))
+
+    def release(self, slot: int):
+        self._check(self.lib.d3q19_pool_release(self.h, slot), "pool_release")
+        self.members.pop(slot, None)
+
+    def usage(self):
+        used, budget, n = C.c_size_t(), C.c_size_t(), C.c_int()
+        self._check(self.lib.d3q19_pool_usage(self.h, C.byref(used), C.byref(budget), C.byref(n)), "pool_usage")
+        return int(used.value), int(budget.value), int(n.value)
+
+    def set_grid(self, fluid_blocks: int, particle_blocks: int, contact_blocks: int):
+        self._check(self.lib.d3q19_pool_set_grid(self.h, fluid_blocks, particle_blocks, contact_blocks), "set_grid")
+
+    def get_grid(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.lib.d3q19_pool_get_grid(self.h, C.byref(a), C.byref(b), C.byref(c)), "get_grid")
+        return a.value, b.value, c.value
+
+    def synchronize(self):
+        self._check(self.lib.d3q19_pool_synchronize(self.h), "pool_synchronize")
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self.lib.d3q19_pool_stream(self.h) or 0)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.d3q19_pool_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def __del__(self):
         try:

@@ -1,0 +1,239 @@
+"""Served shear-rheology solves on one GPU: a request loop over the lattice
+pool (continuous batching), and the one-at-a-time baseline it is measured
+against.
+
+A request is an independent shear cell: a cubic lattice with velocity walls
+on z, periodic x and y, a viscosity law and a suspension of spheres.  It runs
+until the domain-averaged shear stress (d3q19_mean_stress, FP64 on the
+device) changes by less than `rel_tol` relative over `check_every` steps, or
+until `max_steps`.
+
+The server admits requests as they arrive, as long as a slot and HBM budget
+are free; every member of the pool advances in the same batched launches, so
+requests that arrive while others run overlap with them on the device, and a
+finished request frees its memory for the queue.  The reference has no
+counterpart (one lattice per process); the physics of each request is the
+reference's.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import time
+
+import numpy as np
+
+from . import HostState, Options, Pool, Simulation, keywords_text, parse_config
+
+MODELS = ("newtonian", "power_law", "casson")
+
+
+@dataclasses.dataclass
+class ShearRequest:
+    """One shear-rheology solve."""
+    rid: int
+    edge: tuple          # lattice size (incl. the 1-node buffer per face)
+    phi: float           # sphere volume fraction
+    model: str           # "newtonian" | "power_law" | "casson"
+    wall_speed: float    # walls at +-wall_speed along x
+    seed: int            # sphere placement seed
+    arrival: float = 0.0  # seconds after the start of the sweep
+    diameter: float = 8.0
+    n_index: float = 0.6  # power-law index
+
+
+def solve_keywords(req: ShearRequest) -> dict:
+    """Input-file keywords (the reference's names, D3Q19-OpenCL.c:31-64, plus
+    the placement and clamp keywords of this implementation) for a request."""
+    N = tuple(int(v) for v in req.edge)
+    r = req.diameter / 2.0
+    # The wall repulsion (z_wall_particle_buffer) acts within r + 2 of a wall,
+    # so markers stay off the wall planes (a marker that crosses one wraps to
+    # the other wall, as in the reference); sphere centres start in the slab
+    # beyond it, and phi is the volume fraction of that slab (random
+    # sequential addition jams near 0.38).
+    zb = r + 2.0
+    slab = (N[0] - 2) * (N[1] - 2) * max(N[2] - 2 - 2 * zb, 0.0)
+    nsph = int(round(req.phi * slab / (4.0 / 3.0 * math.pi * r ** 3)))
+    kw = dict(iterations=1_000_000, total_lattice_size=N, boundary_conditions_xyz=(0, 0, 1),
+              velocity_bc_upper=(req.wall_speed, 0.0, 0.0), velocity_bc_lower=(-req.wall_speed, 0.0, 0.0),
+              initial_f="constant", initial_vel=(0.0, 0.0, 0.0), domain_decomposition=(1, 1, 1),
+              rebuild_neigh_list_freq=10, video_freq=10 ** 9, shear_stress_freq=10 ** 9, console_print_freq=10 ** 9,
+              num_particles=nsph)
+    if nsph > 0:
+        kw.update(particle_diameter=req.diameter, initial_particle_distribution=4, particle_seed=req.seed,
+                  min_particle_gap=0.0, initial_particle_buffer=0.0, z_wall_particle_buffer=zb,
+                  particle_collision_params=2.0)
+    if req.model == "newtonian":
+        kw.update(newtonian_tau=0.8, viscosity_model=1)
+    elif req.model == "power_law":
+        # Consistency k such that tau = 1 at the nominal shear rate 2U/H.
+        rate = 2.0 * req.wall_speed / (N[2] - 2)
+        k = (1.0 - 0.5) / 3.0 / rate ** (req.n_index - 1.0)
+        kw.update(newtonian_tau=1.0, viscosity_model=2, viscosity_params=(k, req.n_index, 0.0, 0.0),
+                  use_constant_viscosity=0, tau_min=0.55, tau_max=2.0)
+    elif req.model == "casson":
+        kw.update(newtonian_tau=0.8, viscosity_model=4, viscosity_params=(1e-4, (0.6 - 0.5) / 3.0, 0.0, 0.0),
+                  use_constant_viscosity=0, casson_regularisation=1e-4, tau_max=2.0)
+    else:
+        raise ValueError(f"unknown model {req.model}")
+    return kw
+
+
+def host_state(req: ShearRequest, data_dir: str = ".") -> HostState:
+    return HostState(parse_config(keywords_text(solve_keywords(req))), data_dir=data_dir)
+
+
+def make_requests(n: int, rate: float, seed: int, edges=(32, 64), phi=(0.0, 0.3), models=MODELS,
+                  wall_speed=0.02, diameter=8.0) -> list:
+    """n requests with Poisson arrivals of mean rate `rate` per second, cubic
+    edges uniform in [edges[0], edges[1]] (even), volume fractions uniform in
+    phi and the viscosity law uniform over `models`; all from one seed."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate) if rate > 0 else 0.0
+        e = int(rng.integers(edges[0] // 2, edges[1] // 2 + 1)) * 2
+        out.append(ShearRequest(rid=i, edge=(e, e, e), phi=float(rng.uniform(*phi)),
+                                model=str(models[int(rng.integers(len(models)))]), wall_speed=wall_speed,
+                                seed=int(rng.integers(1, 2 ** 31 - 1)), arrival=t, diameter=diameter))
+    return out
+
+
+@dataclasses.dataclass
+class SolveRecord:
+    rid: int
+    arrival: float
+    start: float
+    finish: float
+    steps: int
+    stress: float
+    eff_viscosity: float
+    converged: bool
+
+    @property
+    def latency(self) -> float:
+        return self.finish - self.arrival
+
+
+class Convergence:
+    """The stop rule: the mean shear stress changes by less than rel_tol
+    (relative) between consecutive checks `check_every` steps apart."""
+
+    def __init__(self, rel_tol: float = 1e-4):
+        self.rel_tol = rel_tol
+        self.last = None
+
+    def update(self, stress: float) -> bool:
+        prev, self.last = self.last, stress
+        if prev is None:
+            return False
+        return abs(stress - prev) <= self.rel_tol * max(abs(stress), 1e-300)
+
+
+def summary(records: list, wall: float) -> dict:
+    lat = np.array([r.latency for r in records], np.float64)
+    return {"solves": len(records), "wall_s": wall, "solves_per_s": len(records) / wall if wall > 0 else None,
+            "p50_latency_s": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p99_latency_s": float(np.percentile(lat, 99)) if len(lat) else None,
+            "converged": int(sum(r.converged for r in records)),
+            "steps": int(sum(r.steps for r in records))}
+
+
+class Server:
+    """Continuous batching over a Pool: admit on arrival while slots and
+    budget last, advance every member `check_every` steps at a time, retire
+    the converged ones."""
+
+    def __init__(self, pool: Pool, check_every: int = 500, rel_tol: float = 1e-4, max_steps: int = 20000,
+                 clock=time.perf_counter, sleep=time.sleep):
+        if check_every % pool.period:
+            raise ValueError(f"check_every must be a multiple of the pool period {pool.period}")
+        self.pool = pool
+        self.check_every = check_every
+        self.rel_tol = rel_tol
+        self.max_steps = max_steps
+        self.clock = clock
+        self.sleep = sleep
+
+    def run(self, requests: list, build=host_state) -> tuple:
+        """Serves the requests (arrival times relative to the call); returns
+        (records in completion order, wall seconds)."""
+        queue = sorted(requests, key=lambda r: r.arrival)
+        t0 = self.clock()
+        active = {}  # slot -> (request, start time, Convergence)
+        joining = {}  # admitted while the pool was running: join the next chunk
+        done = []
+        qi = 0
+
+        def admit_arrived():
+            # Admit in arrival order; stop at the first one that does not fit.
+            nonlocal qi
+            while qi < len(queue) and queue[qi].arrival <= self.clock() - t0:
+                req = queue[qi]
+                slot = self.pool.admit(build(req))
+                if slot is None:
+                    if not active and not joining:
+                        raise RuntimeError(f"request {req.rid} does not fit an empty pool")
+                    return
+                joining[slot] = (req, self.clock() - t0, Convergence(self.rel_tol))
+                qi += 1
+
+        while qi < len(queue) or active or joining:
+            admit_arrived()
+            active.update(joining)
+            joining.clear()
+            if not active:
+                self.sleep(max(0.0, queue[qi].arrival - (self.clock() - t0)))
+                continue
+            # The chunk runs on the pool's stream while the host admits the
+            # requests that arrived meanwhile (their set-up and first steps
+            # overlap the chunk on the device); they join the next chunk.
+            self.pool.advance(self.check_every)
+            admit_arrived()
+            for slot in list(active):
+                req, start, conv = active[slot]
+                m = self.pool.member(slot)
+                stress, _, visc = m.mean_stress()
+                steps = self.pool.steps(slot)
+                ok = conv.update(stress)
+                if ok or steps >= self.max_steps:
+                    done.append(SolveRecord(req.rid, req.arrival, start, self.clock() - t0, steps, stress, visc, ok))
+                    self.pool.release(slot)
+                    del active[slot]
+        return done, self.clock() - t0
+
+
+def one_at_a_time(requests: list, storage: int = 0, check_every: int = 500, rel_tol: float = 1e-4,
+                  max_steps: int = 20000, device: int = 0, clock=time.perf_counter, sleep=time.sleep,
+                  build=host_state) -> tuple:
+    """The baseline: each request alone on the GPU, in arrival order (FP32 by
+    default), with the same stop rule."""
+    queue = sorted(requests, key=lambda r: r.arrival)
+    t0 = clock()
+    done = []
+    for req in queue:
+        wait = req.arrival - (clock() - t0)
+        if wait > 0:
+            sleep(wait)
+        start = clock() - t0
+        hs = build(req)
+        sim = Simulation.from_host_state(hs, device=device, storage=storage)
+        conv = Convergence(rel_tol)
+        t, ok = 1, False
+        stress = visc = 0.0
+        while t - 1 < max_steps:
+            sim.run(t, check_every)
+            t += check_every
+            stress, _, visc = sim.mean_stress()
+            if conv.update(stress):
+                ok = True
+                break
+        sim.close()
+        done.append(SolveRecord(req.rid, req.arrival, start, clock() - t0, t - 1, stress, visc, ok))
+    return done, clock() - t0
+
+
+__all__ = ["ShearRequest", "SolveRecord", "Convergence", "Server", "make_requests", "solve_keywords", "host_state",
+           "one_at_a_time", "summary", "MODELS", "Options"]

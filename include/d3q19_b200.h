@@ -74,7 +74,8 @@ enum d3q19_status {
   D3Q19_ENODEV = -4,    /* no usable sm_100 device */
   D3Q19_EOVERFLOW = -5, /* a lattice tile received more IBM markers than its list holds */
   D3Q19_ENUMERIC = -6,  /* non-finite density or velocity detected on the device */
-  D3Q19_ESTATE = -7     /* call out of order (e.g. step before the lattice is written) */
+  D3Q19_ESTATE = -7,    /* call out of order (e.g. step before the lattice is written) */
+  D3Q19_EBUSY = -8      /* the pool has no free slot or HBM budget for the request right now */
 };
 
 /* Options with no counterpart in the reference's parameter structs.  A
@@ -220,6 +221,26 @@ int d3q19_read_marker_cells(d3q19_ctx* ctx, int* cells);
 /* Zone lists after the last rebuild (update_particle_zones). */
 int d3q19_read_zones(d3q19_ctx* ctx, int* parsZone, int* zoneMembers, int* numParInZone);
 
+/* Sums over every z-plane of the interior nodes, in FP64 on the device (no
+ * read-back of the field): out[5*z + 0..2] = sums of u_x, u_y, u_z,
+ * out[5*z + 3] = sum of the shear rate du_x/dz + du_z/dx, out[5*z + 4] = sum
+ * of the viscous shear stress nu*(du_x/dz + du_z/dx), nu = (tau - 1/2)/3.
+ * Central differences, wrapped on periodic axes, one-sided on the wall
+ * layers.  out holds 5*LatticeSize[2] doubles (planes 0 and Nz-1 are 0).
+ * Device-side form of the averages compute_shear_stress takes on the host
+ * (D3Q19-OpenCL.c:670-747). */
+int d3q19_plane_stats(d3q19_ctx* ctx, double* out);
+/* compute_shear_stress (D3Q19-OpenCL.c:670-747) from the device sums:
+ * u_mean[3*z + d] the x-y mean of u_d on plane z (3*Nz doubles, may be
+ * NULL), the wall shear rate (forward differences over 4 planes at both
+ * walls) and the shear rate across the particle region.  FP64 where the
+ * reference accumulates in float. */
+int d3q19_shear_profile(d3q19_ctx* ctx, double* u_mean, double* wall_rate, double* region_rate);
+/* Domain means over the interior nodes, FP64: the viscous shear stress
+ * <nu (du_x/dz + du_z/dx)>, the shear rate <du_x/dz + du_z/dx> and the
+ * effective viscosity (their ratio).  No counterpart in the reference. */
+int d3q19_mean_stress(d3q19_ctx* ctx, double* stress_xz, double* shear_rate, double* eff_viscosity);
+
 /* Number of lattice nodes whose local tau was clamped to 0.505 since the
  * context was created (the reference prints a device warning instead,
  * GPU_program.cl:1071-1074). */
@@ -244,6 +265,64 @@ const char* d3q19_last_error(d3q19_ctx* ctx);
 
 /* Replaces clRelease* (sim_main.c:503-525). */
 int d3q19_destroy(d3q19_ctx* ctx);
+
+/* ---------------------------------------------------------------------------
+ * The lattice pool: many independent shear cells resident on one GPU and
+ * advanced together.  No counterpart in the reference (it runs one lattice
+ * per process); the members are ordinary contexts (same layouts, same
+ * read-backs through d3q19_pool_context) whose steps run in batched
+ * persistent kernels over packed work lists -- one launch per kernel of the
+ * step for all members, captured as CUDA graphs per chunk length.
+ *
+ * Members: periodic x and y with velocity walls on z, the fast arithmetic
+ * with the reference's MRT, the pool's storage format and zone rebuild
+ * period; each keeps its own viscosity law and parameters, lattice size,
+ * spheres and markers.  A member's results do not depend on the other
+ * members.
+ * ------------------------------------------------------------------------- */
+typedef struct d3q19_pool d3q19_pool;
+
+/* Device memory d3q19_create allocates for these parameters (read-back
+ * scratch, allocated on first use, not included). */
+int d3q19_context_bytes(const int_param_struct* ip, const d3q19_options* opt, size_t* bytes);
+/* A pool on `device` for members with distribution storage `storage`
+ * (d3q19_options.storage) and zone rebuild period rebuild_freq; at most
+ * max_slots members whose d3q19_context_bytes sum to at most hbm_budget. */
+int d3q19_pool_create(int device, int storage, int rebuild_freq, int max_slots, size_t hbm_budget,
+                      d3q19_pool** out);
+/* Admits one solve: creates its context from the parameter blocks and the
+ * host arrays of d3q19_write_lattice / _particles / _zones (particle and zone
+ * arrays may be NULL without spheres), runs its first period =
+ * lcm(2, rebuild_freq) steps alone, and makes it a member (its slot in
+ * *slot).  D3Q19_EBUSY when no slot is free or its memory would exceed the
+ * budget now; D3Q19_EINVAL for a solve the pool cannot run. */
+int d3q19_pool_admit(d3q19_pool* pool, const int_param_struct* ip, const flp_param_struct* fp,
+                     const d3q19_options* opt, const float* f, const float* u, const float* tau_lb,
+                     const float* parKin, const float* parForce, const float* parFluidForce,
+                     const float* spherePoints, const int* zoneNeighDat, const int* parsZone,
+                     const int* zoneMembers, const int* numParInZone, int* slot);
+/* Advances every member by nsteps (a positive multiple of the period),
+ * asynchronously on the pool's stream. */
+int d3q19_pool_advance(d3q19_pool* pool, int nsteps);
+/* The member's context, for its read-backs and diagnostics (ordered after the
+ * pool's work); NULL for a free slot.  Do not step it directly. */
+d3q19_ctx* d3q19_pool_context(d3q19_pool* pool, int slot);
+/* Steps the member has taken, or -1 for a free slot. */
+long long d3q19_pool_slot_steps(d3q19_pool* pool, int slot);
+/* Frees the member's slot and device memory. */
+int d3q19_pool_release(d3q19_pool* pool, int slot);
+/* Budget in use, the budget, and the member count. */
+int d3q19_pool_usage(d3q19_pool* pool, size_t* used, size_t* budget, int* members);
+/* Persistent grid sizes (CTAs) of the batched fluid, particle and contact
+ * passes; the autotuner sets them.  Results do not depend on them. */
+int d3q19_pool_set_grid(d3q19_pool* pool, int fluid_blocks, int particle_blocks, int contact_blocks);
+int d3q19_pool_get_grid(d3q19_pool* pool, int* fluid_blocks, int* particle_blocks, int* contact_blocks);
+/* Waits for the pool's work and reports the members' device errors. */
+int d3q19_pool_synchronize(d3q19_pool* pool);
+/* The pool's CUDA stream (cudaStream_t). */
+void* d3q19_pool_stream(d3q19_pool* pool);
+const char* d3q19_pool_last_error(d3q19_pool* pool);
+int d3q19_pool_destroy(d3q19_pool* pool);
 
 #ifdef __cplusplus
 }

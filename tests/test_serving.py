@@ -1,0 +1,125 @@
+"""Host logic of the served sweep (no GPU): request generation, the stop
+rule, and the continuous-batching loop driven against a fake pool that
+counts steps and models the HBM budget."""
+import numpy as np
+import pytest
+
+import d3q19_b200 as d3
+from d3q19_b200 import serving as sv
+
+
+def test_requests_are_seeded_and_poisson():
+    a = sv.make_requests(400, 50.0, 11)
+    b = sv.make_requests(400, 50.0, 11)
+    assert [(r.edge, r.phi, r.model, r.seed, r.arrival) for r in a] == \
+        [(r.edge, r.phi, r.model, r.seed, r.arrival) for r in b]
+    gaps = np.diff([0.0] + [r.arrival for r in a])
+    assert gaps.mean() == pytest.approx(1 / 50.0, rel=0.15)
+    assert all(32 <= r.edge[0] <= 64 and r.edge[0] % 2 == 0 for r in a)
+    assert {r.model for r in a} == set(sv.MODELS)
+    assert all(0.0 <= r.phi <= 0.3 for r in a)
+
+
+@pytest.mark.parametrize("model", sv.MODELS)
+def test_request_builds_reference_initial_state(model):
+    req = sv.ShearRequest(rid=0, edge=(34, 34, 34), phi=0.2, model=model, wall_speed=0.02, seed=5)
+    hs = sv.host_state(req)
+    ip = hs.cfg.ip
+    assert tuple(ip.LatticeSize) == (34, 34, 34) and tuple(ip.BoundaryConds) == (0, 0, 1)
+    assert ip.NumParticles > 0
+    assert ip.ViscosityModel == {"newtonian": 1, "power_law": 2, "casson": 4}[model]
+    assert hs.options.variable_viscosity == (model != "newtonian")
+    z = hs.parKin.reshape(-1, 4)[:ip.NumParticles, 2]
+    assert np.all(z >= 6.0) and np.all(z <= 32.0 - 6.0)  # radius + 2 off the walls
+    assert hs.cfg.fp.ParticleZBuffer == 6.0
+
+
+def test_stop_rule():
+    c = sv.Convergence(1e-4)
+    assert not c.update(1.0)
+    assert not c.update(1.001)
+    assert c.update(1.00105)
+
+
+class FakeMember:
+    def __init__(self, pool, slot, target):
+        self.pool, self.slot, self.target = pool, slot, target
+
+    def mean_stress(self):
+        s = self.pool.steps_done[self.slot]
+        # Relaxes towards the target: converges after a request-dependent time.
+        return self.target * (1.0 - np.exp(-s / 1000.0)), 0.0, 0.0
+
+
+class FakePool:
+    period = 10
+
+    def __init__(self, budget):
+        self.budget, self.used = budget, 0
+        self.steps_done, self.size, self.target = {}, {}, {}
+        self.admitted, self.max_members, self.next = [], 0, 0
+
+    def admit(self, hs):
+        b = hs["bytes"]
+        if self.used + b > self.budget:
+            return None
+        s = self.next
+        self.next += 1
+        self.used += b
+        self.size[s], self.steps_done[s], self.target[s] = b, self.period, hs["target"]
+        self.admitted.append(hs["rid"])
+        self.max_members = max(self.max_members, len(self.size))
+        return s
+
+    def advance(self, n):
+        for s in self.size:
+            self.steps_done[s] += n
+
+    def member(self, s):
+        return FakeMember(self, s, self.target[s])
+
+    def steps(self, s):
+        return self.steps_done[s]
+
+    def release(self, s):
+        self.used -= self.size.pop(s)
+
+
+def test_server_admits_in_order_within_budget_and_retires():
+    # A burst: all twelve are waiting from the start.
+    reqs = [sv.ShearRequest(rid=i, edge=(32, 32, 32), phi=0.0, model="newtonian", wall_speed=0.02, seed=1,
+                            arrival=1e-6 * i) for i in range(12)]
+    pool = FakePool(budget=4 * 10)
+    clock = {"t": 0.0}
+
+    def now():
+        clock["t"] += 1e-4
+        return clock["t"]
+
+    srv = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=30000, clock=now,
+                    sleep=lambda dt: clock.__setitem__("t", clock["t"] + dt))
+    build = lambda r: {"bytes": 10, "rid": r.rid, "target": 1.0 + r.rid}
+    recs, wall = srv.run(reqs, build=build)
+    assert sorted(r.rid for r in recs) == list(range(12))
+    assert pool.admitted == list(range(12))  # arrival order
+    assert pool.max_members == 4             # the budget holds 4 at a time
+    assert pool.used == 0
+    assert all(r.converged for r in recs)
+    assert all(r.finish >= r.start >= r.arrival for r in recs)
+    s = sv.summary(recs, wall)
+    assert s["solves"] == 12 and s["p99_latency_s"] >= s["p50_latency_s"] > 0
+
+
+def test_server_rejects_check_interval_off_the_period():
+    with pytest.raises(ValueError):
+        sv.Server(FakePool(10), check_every=505)
+
+
+def test_context_bytes_counts_the_distributions():
+    cfg = d3.parse_config("total_lattice_size 64 64 64\nboundary_conditions_xyz 0 0 1\nnum_particles 0\n")
+    b32 = d3.context_bytes(cfg.ip, d3.Options())
+    o = d3.Options()
+    o.storage = 1
+    b16 = d3.context_bytes(cfg.ip, o)
+    nc = 64 ** 3
+    assert b32 >= 2 * 19 * 4 * nc + 16 * nc and b32 - b16 == pytest.approx(2 * 19 * 2 * nc, rel=1e-3)
