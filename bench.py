@@ -534,6 +534,69 @@ def run_served(args):
                                                                "median": float(np.median(visc_err))}}
 
 
+def run_precision(args):
+    """Casson suspension: 256x128x256 lattice, 1000 spheres of radius 6 (384
+    markers each, seeded random placement), regularised Casson yield stress
+    1e-4 and plastic tau 0.6, walls +-0.04; FP32, FP16 and BF16 shifted
+    storage against the FP64 build after the same steps: errors of velocity,
+    mean shear stress, effective viscosity and per-sphere force and torque."""
+    import numpy as np
+    import torch
+
+    import d3q19_b200 as d3
+
+    torch.cuda.set_device(0)
+    kw = dict(iterations=args.steps, total_lattice_size=(256, 128, 256), boundary_conditions_xyz=(0, 0, 1),
+              newtonian_tau=0.6, viscosity_model=4, viscosity_params=(1e-4, (0.6 - 0.5) / 3.0, 0.0, 0.0),
+              use_constant_viscosity=0, casson_regularisation=1e-4, velocity_bc_upper=(0.04, 0.0, 0.0),
+              velocity_bc_lower=(-0.04, 0.0, 0.0), initial_f="constant", initial_vel=(0.0, 0.0, 0.0),
+              num_particles=1000, particle_diameter=12.0, ibm_points_per_particle=384,
+              initial_particle_distribution=4, particle_seed=1, min_particle_gap=1.0, initial_particle_buffer=0.0,
+              z_wall_particle_buffer=8.0, domain_decomposition=(1, 1, 1), rebuild_neigh_list_freq=10,
+              particle_collision_params=2.0, video_freq=10 ** 9, shear_stress_freq=10 ** 9,
+              console_print_freq=10 ** 9)
+    hs = d3.HostState(d3.parse_config(d3.keywords_text(kw)), data_dir=os.getcwd())
+    ip = hs.cfg.ip
+    n = args.steps
+    interior = (ip.LatticeSize[0] - 2) * (ip.LatticeSize[1] - 2) * (ip.LatticeSize[2] - 2)
+    out = {}
+    for label, over in (("fp64", dict(arithmetic=2)), ("fp32", {}), ("fp16", dict(storage=1)),
+                        ("bf16", dict(storage=2))):
+        sim = d3.Simulation.from_host_state(hs, device=0, **over)
+        stream = torch.cuda.ExternalStream(sim.stream_ptr)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.run(1, n)
+        e1.record(stream)
+        sim.synchronize()
+        ms = e0.elapsed_time(e1)
+        np_ = ip.NumParticles
+        pff = sim.read_parfluidforce().reshape(2, np_, ip.WorkGroupsPerParticle, 4).astype(np.float64).sum(axis=2)
+        out[label] = dict(u=sim.read_u().astype(np.float64), stress=sim.mean_stress(), pff=pff[:, :, :3],
+                          mlups=interior * n / (ms * 1e-3) / 1e6)
+        sim.close()
+    ref = out["fp64"]
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    table = {}
+    for label in ("fp32", "fp16", "bf16"):
+        o = out[label]
+        table[label] = {"u_rel_l2": rel(o["u"], ref["u"]),
+                        "mean_stress_rel": abs(o["stress"][0] - ref["stress"][0]) / abs(ref["stress"][0]),
+                        "eff_viscosity_rel": abs(o["stress"][2] - ref["stress"][2]) / abs(ref["stress"][2]),
+                        "sphere_force_rel_l2": rel(o["pff"][0], ref["pff"][0]),
+                        "sphere_torque_rel_l2": rel(o["pff"][1], ref["pff"][1]),
+                        "mlups": round(o["mlups"], 1)}
+    return {"metric": "error vs FP64 build", "impl": "ours", "n_gpus": 1, "steps": n,
+            "config": {"workload": "casson-256x128x256", "spheres": ip.NumParticles,
+                       "markers_per_sphere": ip.PointsPerParticle,
+                       "description": "regularised Casson (tau_Y 1e-4, plastic tau 0.6), 1000 spheres r=6, "
+                                      "walls +-0.04"},
+            "fp64_mlups": round(ref["mlups"], 1), "fp64_eff_viscosity": ref["stress"][2], "errors": table}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -541,7 +604,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dense-powerlaw-128", choices=sorted(WORKLOADS) + ["batch-64",
-                                                                                           "served-sweep"])
+                                                                                           "served-sweep",
+                                                                                           "casson-precision"])
     ap.add_argument("--requests", type=int, default=128, help="served-sweep: number of requests")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", default="fp32", choices=sorted(STORAGE),
@@ -556,9 +620,10 @@ def main():
         if rank == 0:
             print(json.dumps(run_reference_arm(args)), flush=True)
         return
-    if args.workload in ("batch-64", "served-sweep"):
+    if args.workload in ("batch-64", "served-sweep", "casson-precision"):
         if rank == 0:
-            print(json.dumps(run_batch(args) if args.workload == "batch-64" else run_served(args)), flush=True)
+            run = {"batch-64": run_batch, "served-sweep": run_served, "casson-precision": run_precision}
+            print(json.dumps(run[args.workload](args)), flush=True)
         return
     dist = None
     if world > 1:

@@ -41,7 +41,12 @@ struct d3q19_ctx {
   int f_state = 0;     // 0 unset, 1 reference state (pre-collision), 2 post-collision
   float* u = nullptr;
   float* tau = nullptr;
+  double* tau64 = nullptr;  // arithmetic = 2: the local tau in double
   float4* kin[2] = {nullptr, nullptr};
+  // particle_precision = 1: sphere state and force/torque partials in double
+  // (the float buffers hold rounded copies for read-back and the contacts).
+  double* kin64[2] = {nullptr, nullptr};
+  double* pff64[2] = {nullptr, nullptr};
   float4* pff[2] = {nullptr, nullptr};
   float4* pf[2] = {nullptr, nullptr};
   int pcur = 0;
@@ -136,7 +141,9 @@ static int validate(const int_param_struct* ip, const flp_param_struct* fp, cons
   if (ip->BoundaryConds[0] + ip->BoundaryConds[1] + ip->BoundaryConds[2] > 1)
     return fail(nullptr, D3Q19_EINVAL, "more than 1 pair of faces with velocity boundaries (D3Q19-OpenCL.c:103)");
   if (o->collision < 0 || o->collision > 1) return fail(nullptr, D3Q19_EINVAL, "collision must be 0 or 1");
-  if (o->arithmetic < 0 || o->arithmetic > 1) return fail(nullptr, D3Q19_EINVAL, "arithmetic must be 0 or 1");
+  if (o->arithmetic < 0 || o->arithmetic > 2) return fail(nullptr, D3Q19_EINVAL, "arithmetic must be 0, 1 or 2");
+  if (o->arithmetic == 2 && (o->collision != 0 || o->storage != 0))
+    return fail(nullptr, D3Q19_EINVAL, "the FP64 build runs the reference's MRT on FP64 distributions only");
   if (o->arithmetic == 1 && o->collision != 0)
     return fail(nullptr, D3Q19_EINVAL, "the reference-exact arithmetic implements the reference's MRT only");
   if (o->arithmetic == 1 && (o->tau_max != 0.0f || o->tau_min != 0.0f || o->casson_reg != 0.0f))
@@ -147,8 +154,10 @@ static int validate(const int_param_struct* ip, const flp_param_struct* fp, cons
     return fail(nullptr, D3Q19_EINVAL, "storage %d (0 FP32, 1 FP16 shifted, 2 BF16 shifted)", o->storage);
   if (o->arithmetic == 1 && o->storage != 0)
     return fail(nullptr, D3Q19_EINVAL, "the reference-exact arithmetic stores FP32 distributions only");
-  if (o->particle_precision != 0)
-    return fail(nullptr, D3Q19_EINVAL, "particle_precision %d not available in this build", o->particle_precision);
+  if (o->particle_precision < 0 || o->particle_precision > 1)
+    return fail(nullptr, D3Q19_EINVAL, "particle_precision %d (0 FP32, 1 FP64)", o->particle_precision);
+  if (o->particle_precision == 1 && o->arithmetic == 1)
+    return fail(nullptr, D3Q19_EINVAL, "the reference-exact arithmetic keeps the reference's FP32 particle state");
   if (fp->NewtonianTau <= 0.5f) return fail(nullptr, D3Q19_EINVAL, "NewtonianTau must exceed 0.5");
   const int np = ip->NumParticles;
   if (np < 0) return fail(nullptr, D3Q19_EINVAL, "NumParticles < 0");
@@ -179,6 +188,10 @@ extern "C" int d3q19_create(const int_param_struct* ip, const flp_param_struct* 
   if (o.rebuild_freq <= 0) o.rebuild_freq = 10;  // the reference's default (D3Q19-OpenCL.c:60)
   int rc = validate(ip, fp, &o);
   if (rc) return rc;
+  if (o.arithmetic == 2) {  // the FP64 build: FP64 distributions and particles
+    o.storage = STORE_F64;
+    o.particle_precision = 1;
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || o.device < 0 || o.device >= ndev)
     return fail(nullptr, D3Q19_ENODEV, "CUDA device %d not available", o.device);
@@ -263,7 +276,7 @@ extern "C" int d3q19_create(const int_param_struct* ip, const flp_param_struct* 
   if ((rc = dalloc(c, (char**)&c->f[0], fbytes)) || (rc = dalloc(c, (char**)&c->f[1], fbytes)) ||
       (rc = dalloc(c, &c->u, 3 * NC)) ||
       (rc = dalloc(c, &c->tau, NC)) || (rc = dalloc(c, &c->err, 1)) || (rc = dalloc(c, &c->clamps, 1)) ||
-      (rc = dalloc(c, &c->pstats, 5LL * g.Nz))) {
+      (rc = dalloc(c, &c->pstats, 5LL * g.Nz)) || (o.arithmetic == 2 && (rc = dalloc(c, &c->tau64, NC)))) {
     snprintf(g_create_error, sizeof(g_create_error), "%s", c->msg);
     d3q19_destroy(c);
     return rc;
@@ -281,6 +294,8 @@ extern "C" int d3q19_create(const int_param_struct* ip, const flp_param_struct* 
       rc = dalloc(c, &c->kin[b], 4 * np);
       if (!rc) rc = dalloc(c, &c->pff[b], 2LL * np * pp.nfa);
       if (!rc) rc = dalloc(c, &c->pf[b], 2 * np);
+      if (!rc && o.particle_precision == 1) rc = dalloc(c, &c->kin64[b], 16 * (long long)np);
+      if (!rc && o.particle_precision == 1) rc = dalloc(c, &c->pff64[b], 8LL * np * pp.nfa);
     }
     if (!rc) rc = dalloc(c, &c->sphere, pp.P);
     if (!rc) rc = dalloc(c, &c->mrec, 2 * M);
@@ -334,6 +349,7 @@ extern "C" int d3q19_write_lattice(d3q19_ctx* c, const float* f, const float* u,
     CUDA_TRY(c, cudaMemcpyAsync(c->tau, t.data(), sizeof(float) * NC, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   }
+  if (c->tau64) CUDA_TRY(c, launch_widen(c->tau, c->tau64, NC, c->stream));
   c->f_state = 1;
   return 0;
 }
@@ -352,6 +368,10 @@ extern "C" int d3q19_write_particles(d3q19_ctx* c, const float* parKin, const fl
                               cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaMemcpyAsync(c->sphere, spherePoints, sizeof(float4) * c->ppar.P, cudaMemcpyHostToDevice,
                               c->stream));
+  if (c->kin64[b]) {
+    CUDA_TRY(c, launch_widen((const float*)c->kin[b], c->kin64[b], 16LL * np, c->stream));
+    CUDA_TRY(c, launch_widen((const float*)c->pff[b], c->pff64[b], 8LL * np * c->ppar.nfa, c->stream));
+  }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->have_particles = true;
   return 0;
@@ -500,6 +520,7 @@ static FluidArgs fluid_args(const d3q19_ctx* c, int t, int cur) {
   fa.fout = c->f[1 - cur];
   fa.u = c->u;
   fa.tau = c->tau;
+  fa.tau64 = c->tau64;
   fa.tiles.cap = c->tile_cap;
   fa.tiles.count = c->tile_count;
   fa.tiles.list = c->tile_list;
@@ -538,6 +559,11 @@ static ParticleArgs particle_args(const d3q19_ctx* c, int t, int pcur) {
   pa.revList = c->revList;
   pa.err = c->err;
   pa.t = t;
+  pa.p64 = c->kin64[0] != nullptr;
+  pa.kin64_old = c->kin64[pcur];
+  pa.kin64_new = c->kin64[1 - pcur];
+  pa.pff64_old = c->pff64[pcur];
+  pa.pff64_new = c->pff64[1 - pcur];
   return pa;
 }
 
@@ -708,6 +734,12 @@ extern "C" int d3q19_read_parkin(d3q19_ctx* c, float* k) {
   if (!c) return D3Q19_EINVAL;
   if (c->ppar.np == 0) return 0;
   return readback(c, (float4*)k, c->kin[c->pcur], 4 * (size_t)c->ppar.np);
+}
+extern "C" int d3q19_read_parkin64(d3q19_ctx* c, double* k) {
+  if (!c) return D3Q19_EINVAL;
+  if (c->ppar.np == 0) return 0;
+  if (!c->kin64[0]) return fail(c, D3Q19_ESTATE, "the particle state is FP32 (particle_precision = 0)");
+  return readback(c, k, (const double*)c->kin64[c->pcur], 16 * (size_t)c->ppar.np);
 }
 extern "C" int d3q19_read_parforce(d3q19_ctx* c, float* k) {
   if (!c) return D3Q19_EINVAL;
@@ -924,7 +956,8 @@ extern "C" int d3q19_destroy(d3q19_ctx* c) {
   drop_events(c);
   void* ptrs[] = {c->f[0], c->f[1], c->u, c->tau, c->kin[0], c->kin[1], c->pff[0], c->pff[1], c->pf[0], c->pf[1],
                   c->sphere, c->mrec, c->tile_count, c->fmax, c->tile_list, c->znd, c->parsZone, c->zoneMembers,
-                  c->numParInZone, c->revStart, c->revList, c->zoneOf, c->err, c->clamps, c->pstats, c->scratch};
+                  c->numParInZone, c->revStart, c->revList, c->zoneOf, c->err, c->clamps, c->pstats, c->scratch,
+                  c->tau64, c->kin64[0], c->kin64[1], c->pff64[0], c->pff64[1]};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1021,18 +1054,24 @@ extern "C" int d3q19_context_bytes(const int_param_struct* ip, const d3q19_optio
   d3q19_options o;
   memset(&o, 0, sizeof(o));
   if (opt) o = *opt;
-  if (o.storage < 0 || o.storage > 2) return D3Q19_EINVAL;
+  if (o.storage < 0 || o.storage > 2 || o.arithmetic < 0 || o.arithmetic > 2) return D3Q19_EINVAL;
+  if (o.arithmetic == 2) {
+    o.storage = STORE_F64;
+    o.particle_precision = 1;
+  }
   const long long NC = (long long)ip->LatticeSize[0] * ip->LatticeSize[1] * ip->LatticeSize[2];
   const long long ntiles = (long long)((ip->LatticeSize[0] + TILE_X - 1) / TILE_X) *
                            ((ip->LatticeSize[1] + TILE_Y - 1) / TILE_Y) * ((ip->LatticeSize[2] + TILE_Z - 1) / TILE_Z);
   size_t b = 2 * round_alloc((size_t)storage_bytes(o.storage) * 19 * NC) + round_alloc(12 * (size_t)NC) +
-             round_alloc(4 * (size_t)NC) + 3 * 512 + round_alloc(40 * (size_t)ip->LatticeSize[2]);
+             round_alloc(4 * (size_t)NC) + 3 * 512 + round_alloc(40 * (size_t)ip->LatticeSize[2]) +
+             (o.arithmetic == 2 ? round_alloc(8 * (size_t)NC) : 0);
   const long long np = ip->NumParticles;
   if (np > 0) {
     const long long P = ip->PointsPerParticle, nfa = ip->WorkGroupsPerParticle, M = np * P;
     const long long Z = (long long)ip->NumZones[0] * ip->NumZones[1] * ip->NumZones[2];
     const long long cap = o.ibm_tile_capacity > 0 ? o.ibm_tile_capacity : std::min<long long>(M, 2048);
     b += 2 * (round_alloc(64 * np) + round_alloc(32 * np * nfa) + round_alloc(32 * np));
+    if (o.particle_precision == 1) b += 2 * (round_alloc(128 * np) + round_alloc(64 * np * nfa));
     b += round_alloc(16 * P) + round_alloc(32 * M) + round_alloc(4 * ntiles) + 512 + round_alloc(4 * ntiles * cap);
     b += round_alloc(4 * 28 * Z) + round_alloc(4 * np) + round_alloc(4 * Z * np) + round_alloc(4 * Z) +
          round_alloc(4 * (Z + 1)) + round_alloc(4 * 27 * Z) + round_alloc(4 * np);
@@ -1146,8 +1185,8 @@ extern "C" int d3q19_pool_admit(d3q19_pool* p, const int_param_struct* ip, const
   o.device = p->dev;
   if (o.storage != p->storage) return pfail(p, D3Q19_EINVAL, "storage %d differs from the pool's %d", o.storage,
                                             p->storage);
-  if (o.arithmetic != 0 || o.collision != 0)
-    return pfail(p, D3Q19_EINVAL, "the pool runs the fast arithmetic with the reference's MRT only");
+  if (o.arithmetic != 0 || o.collision != 0 || o.particle_precision != 0)
+    return pfail(p, D3Q19_EINVAL, "the pool runs the fast FP32 arithmetic with the reference's MRT only");
   if (ip->BoundaryConds[0] != 0 || ip->BoundaryConds[1] != 0 || ip->BoundaryConds[2] != 1 ||
       o.tangential_vel_bc[0] || o.tangential_vel_bc[1] || o.tangential_vel_bc[2])
     return pfail(p, D3Q19_EINVAL, "the pool runs shear cells: periodic x and y, velocity walls on z");

@@ -78,6 +78,7 @@ struct FluidArgs {
   void* fout;
   float* u;
   float* tau;
+  double* tau64;  // local tau of the FP64 build (tau holds its float copy)
   TileLists tiles;
   int has_ibm;
   unsigned* err;
@@ -123,6 +124,13 @@ struct ParticleArgs {
   const int* revList;
   unsigned* err;
   int t;
+  // particle_precision = 1: the sphere state and the force/torque partials in
+  // double (layouts of kin and pff with double components).
+  int p64;
+  const double* kin64_old;
+  double* kin64_new;
+  const double* pff64_old;
+  double* pff64_new;
 };
 
 struct ZoneArgs {
@@ -137,8 +145,9 @@ struct ZoneArgs {
 
 // Launchers (d3q19_kernels.cu).
 // Storage of the distributions: 0 float, 1 half (f - w), 2 bfloat16 (f - w).
-constexpr int STORE_F32 = 0, STORE_F16 = 1, STORE_BF16 = 2;
-inline int storage_bytes(int storage) { return storage == STORE_F32 ? 4 : 2; }
+// STORE_F64 is internal: the FP64 build (d3q19_options.arithmetic = 2).
+constexpr int STORE_F32 = 0, STORE_F16 = 1, STORE_BF16 = 2, STORE_F64 = 3;
+inline int storage_bytes(int storage) { return storage == STORE_F32 ? 4 : (storage == STORE_F64 ? 8 : 2); }
 
 cudaError_t launch_fluid(const FluidArgs& a, bool first, bool variable, int collision, int storage, cudaStream_t s);
 cudaError_t launch_materialize_f(const FluidArgs& a, int storage, float* out, cudaStream_t s);
@@ -146,6 +155,8 @@ cudaError_t launch_materialize_f(const FluidArgs& a, int storage, float* out, cu
 // row q of each N_C-long row block shifted by w_q).
 cudaError_t launch_store_f(const float* in, void* out, long long NC, int storage, cudaStream_t s);
 cudaError_t launch_load_f(const void* in, float* out, long long NC, int storage, cudaStream_t s);
+// out[k] = in[k] for n values (float to double).
+cudaError_t launch_widen(const float* in, double* out, long long n, cudaStream_t s);
 // The particle pass (rigid bodies, IBM interpolation and marker lists) and
 // the particle-particle forces from the positions it wrote.
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s);

@@ -59,18 +59,61 @@ namespace d3q19 {
 // the shifted value f_q - w_q (w_q the rest-state weight 1/3, 1/18, 1/36),
 // whose magnitude is a small fraction of w_q, so the 16-bit significand
 // spends its bits on the deviation from rest.  Arithmetic stays FP32; the
-// stored value is rounded to nearest even once per step.
+// stored value is rounded to nearest even once per step.  ST = double is the
+// FP64 build (arithmetic in double as well).
 #define WQ(q) ((q) == 0 ? (1.0f / 3.0f) : (q) <= 6 ? (1.0f / 18.0f) : (1.0f / 36.0f))
+// The same weights in the arithmetic type R.
+template <typename R>
+__device__ __forceinline__ constexpr R wq(int q) {
+  return q == 0 ? R(1) / R(3) : (q <= 6 ? R(1) / R(18) : R(1) / R(36));
+}
+
+// Arithmetic type of a storage type: FP32 for float and the 16-bit forms,
+// FP64 for double (the FP64 build of the collide-stream kernel).
+template <typename ST>
+struct RealOf {
+  using type = float;
+};
+template <>
+struct RealOf<double> {
+  using type = double;
+};
+
+// Functions of the collide-stream arithmetic: FP32 uses the hardware
+// approximations of the reciprocal, reciprocal square root and power (a few
+// ulp); FP64 evaluates them in double.
+template <typename R>
+struct RMath;
+template <>
+struct RMath<float> {
+  static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
+  static __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+  static __device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
+  static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
+  static __device__ __forceinline__ float pow(float x, float e) { return exp2f(__log2f(x) * e); }
+};
+template <>
+struct RMath<double> {
+  static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+  static __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+  static __device__ __forceinline__ double rsqrt(double x) { return ::rsqrt(x); }
+  static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
+  static __device__ __forceinline__ double pow(double x, double e) { return ::pow(x, e); }
+};
 
 template <typename ST>
 struct Stored;
-// load/store take and give f_q; load_dev/store_dev the deviation f_q - w_q.
+// load/store take and give f_q (the 16-bit forms through load_dev and
+// store_dev, which give and take the stored deviation f_q - w_q).
 template <>
 struct Stored<float> {
   static __device__ __forceinline__ float load(const float* p, float) { return __ldg(p); }
   static __device__ __forceinline__ void store(float* p, float v, float) { *p = v; }
-  static __device__ __forceinline__ float load_dev(const float* p, float w) { return __ldg(p) - w; }
-  static __device__ __forceinline__ void store_dev(float* p, float d, float w) { *p = d + w; }
+};
+template <>
+struct Stored<double> {
+  static __device__ __forceinline__ double load(const double* p, double) { return __ldg(p); }
+  static __device__ __forceinline__ void store(double* p, double v, double) { *p = v; }
 };
 template <>
 struct Stored<__half> {
@@ -99,103 +142,101 @@ struct Stored<__nv_bfloat16> {
 // inward normal +A; SIDE 1 = upper), rho = 1, the inward normal velocity
 // follows from the knowns, and each unknown is its opposite population plus
 // rho*(u_n + c_t.u_t)/6, or rho*u_n/3 for the normal direction.
-// DEV: f holds deviations from the rest state, f_q - w_q (the weights of the
-// 9 tangential and the 5 outgoing populations sum to 2/3 and 1/6, so
-// 1 - (sum9 + 2 sum5) becomes -(sum9 + 2 sum5); unknown and opposite
-// population share w_q).
-template <int A, int SIDE, bool DEV = false>
-__device__ __forceinline__ void velocity_bc(float (&f)[19], const float* uw) {
+template <int A, int SIDE, typename R>
+__device__ __forceinline__ void velocity_bc(R (&f)[19], const float* uw) {
   constexpr int IN = SIDE == 0 ? 1 : -1;
   constexpr int A1 = A == 0 ? 1 : 0;
   constexpr int A2 = A == 2 ? 1 : 2;
-  float sum9 = 0.0f, sum5 = 0.0f;
+  R sum9 = R(0), sum5 = R(0);
 #pragma unroll
   for (int q = 0; q < 19; q++) {
     if (CAQ(A, q) == 0) sum9 += f[q];
     else if (CAQ(A, q) == -IN) sum5 += f[q];
   }
-  const float rho = 1.0f;
-  const float un = DEV ? -(sum9 + 2.0f * sum5) : 1.0f - (sum9 + 2.0f * sum5) / rho;
-  const float ua1 = uw[A1], ua2 = uw[A2];
+  const R rho = R(1);
+  const R un = R(1) - (sum9 + R(2) * sum5) / rho;
+  const R ua1 = uw[A1], ua2 = uw[A2];
 #pragma unroll
   for (int q = 1; q < 19; q++) {
     if (CAQ(A, q) != IN) continue;
     const int t1 = CAQ(A1, q), t2 = CAQ(A2, q);
-    float v;
+    R v;
     if (t1 == 0 && t2 == 0) {
-      v = f[OPPQ(q)] + rho * un / 3.0f;
+      v = f[OPPQ(q)] + rho * un / R(3);
     } else if (t1 != 0) {
-      v = f[OPPQ(q)] + rho * (t1 > 0 ? un + ua1 : un - ua1) / 6.0f;
+      v = f[OPPQ(q)] + rho * (t1 > 0 ? un + ua1 : un - ua1) / R(6);
     } else {
-      v = f[OPPQ(q)] + rho * (t2 > 0 ? un + ua2 : un - ua2) / 6.0f;
+      v = f[OPPQ(q)] + rho * (t2 > 0 ? un + ua2 : un - ua2) / R(6);
     }
     f[q] = v;
   }
 }
 
-template <bool DEV = false>
-__device__ __forceinline__ void apply_wall(float (&f)[19], int axis, int side, const FluidParams& p) {
+template <typename R>
+__device__ __forceinline__ void apply_wall(R (&f)[19], int axis, int side, const FluidParams& p) {
   const float* uw = side ? p.velUpper : p.velLower;
   if (axis == 0) {
-    if (side) velocity_bc<0, 1, DEV>(f, uw); else velocity_bc<0, 0, DEV>(f, uw);
+    if (side) velocity_bc<0, 1>(f, uw); else velocity_bc<0, 0>(f, uw);
   } else if (axis == 1) {
-    if (side) velocity_bc<1, 1, DEV>(f, uw); else velocity_bc<1, 0, DEV>(f, uw);
+    if (side) velocity_bc<1, 1>(f, uw); else velocity_bc<1, 0>(f, uw);
   } else {
-    if (side) velocity_bc<2, 1, DEV>(f, uw); else velocity_bc<2, 0, DEV>(f, uw);
+    if (side) velocity_bc<2, 1>(f, uw); else velocity_bc<2, 0>(f, uw);
   }
 }
 
-// Local relaxation time (GPU_program.cl:1041-1128), with the hardware
-// approximations of the reciprocal, reciprocal square root and power
-// (a few ulp; the reference-exact arithmetic evaluates them as written).
-// Optional extensions: an upper clamp and a regularised Casson yield term.
-// VISC is the viscosity law fixed at compile time (2 power law, 3
-// Herschel-Bulkley, 4 Casson), or -1 to read it from p.viscModel.
-template <int VISC = -1>
-__device__ __forceinline__ float compute_tau(const FluidParams& p, float srt, bool& clamped) {
-  float tau = p.tauN;
-  const float eps = 1e-8f;
+// Local relaxation time (GPU_program.cl:1041-1128).  FP32 uses the hardware
+// approximations of the reciprocal, reciprocal square root and power (a few
+// ulp; the reference-exact arithmetic evaluates them as written), FP64 the
+// double functions.  Optional extensions: an upper clamp and a regularised
+// Casson yield term.  VISC is the viscosity law fixed at compile time (2
+// power law, 3 Herschel-Bulkley, 4 Casson), or -1 to read it from
+// p.viscModel.
+template <int VISC = -1, typename R = float>
+__device__ __forceinline__ R compute_tau(const FluidParams& p, R srt, bool& clamped) {
+  using M = RMath<R>;
+  R tau = p.tauN;
+  const R eps = R(1e-8f);
   const int model = VISC >= 0 ? VISC : p.viscModel;
   if (model == 2) {  // power law
-    float k = p.visc[0], n = p.visc[1], nu;
+    R k = p.visc[0], n = p.visc[1], nu;
     srt = srt > eps ? srt : eps;
-    if (n == 0.5f) nu = k * rsqrtf(srt);
-    else if (n == 1.0f) nu = k;
-    else if (n == 2.0f) nu = k * srt;
-    else nu = k * exp2f(__log2f(srt) * (n - 1.0f));
-    tau = 3.0f * nu + 0.5f;
+    if (n == R(0.5f)) nu = k * M::rsqrt(srt);
+    else if (n == R(1)) nu = k;
+    else if (n == R(2)) nu = k * srt;
+    else nu = k * M::pow(srt, n - R(1));
+    tau = R(3) * nu + R(0.5f);
   } else if (model == 4) {  // Casson
-    float tY = p.visc[0], eta = p.visc[1];
+    R tY = p.visc[0], eta = p.visc[1];
     srt = srt > eps ? srt : eps;
-    float sr2 = p.cassonReg > 0.0f ? srt * srt + p.cassonReg * p.cassonReg : srt * srt;
-    float a = sqrtf(tY * rsqrtf(sr2)) + sqrtf(eta);
-    tau = 3.0f * (a * a) + 0.5f;
+    R sr2 = p.cassonReg > 0.0f ? srt * srt + R(p.cassonReg) * R(p.cassonReg) : srt * srt;
+    R a = M::sqrt(tY * M::rsqrt(sr2)) + M::sqrt(eta);
+    tau = R(3) * (a * a) + R(0.5f);
   } else if (model == 3) {  // Herschel-Bulkley
-    float tY = p.visc[0], k = p.visc[1], n = p.visc[2], nu;
+    R tY = p.visc[0], k = p.visc[1], n = p.visc[2], nu;
     srt = srt > eps ? srt : eps;
-    const float yield = __fdividef(tY, srt);
-    if (n == 0.5f) nu = yield + k * rsqrtf(srt);
-    else if (n == 1.0f) nu = yield + k;
-    else if (n == 2.0f) nu = yield + k * srt;
-    else nu = yield + k * exp2f(__log2f(srt) * (n - 1.0f));
-    tau = 3.0f * nu + 0.5f;
+    const R yield = M::fdiv(tY, srt);
+    if (n == R(0.5f)) nu = yield + k * M::rsqrt(srt);
+    else if (n == R(1)) nu = yield + k;
+    else if (n == R(2)) nu = yield + k * srt;
+    else nu = yield + k * M::pow(srt, n - R(1));
+    tau = R(3) * nu + R(0.5f);
   } else {
     return tau;
   }
   clamped = false;
   if (p.tauMin > 0.0f) {
-    if (tau < p.tauMin) {
+    if (tau < R(p.tauMin)) {
       tau = p.tauMin;
       clamped = true;
     }
-  } else if (tau <= 0.505f) {
+  } else if (sizeof(R) == 4 ? tau <= R(0.505f) : tau < R(0.505)) {
     // The reference compares with the double constant MIN_TAU = 0.505
     // (GPU_program.cl:6); (double)tau < 0.505 holds exactly for the floats
     // up to and including 0.505f, which lies below 0.505.
-    tau = 0.505f;
+    tau = sizeof(R) == 4 ? R(0.505f) : R(0.505);
     clamped = true;
   }
-  if (p.tauMax > 0.0f && tau > p.tauMax) tau = p.tauMax;
+  if (p.tauMax > 0.0f && tau > R(p.tauMax)) tau = p.tauMax;
   return tau;
 }
 
@@ -206,15 +247,15 @@ __device__ __forceinline__ float compute_tau(const FluidParams& p, float srt, bo
 // Addressing: row q of the distributions starts at fin + q*NC (a 64-bit
 // offset, the same for every thread); within a row the node index is a
 // 32-bit int (N_C < 2^31 is checked when the context is created).
-template <typename ST, bool DEV = false>
-__device__ __forceinline__ void gather(float (&f)[19], const ST* __restrict__ fin, long long NC, int i, int dxm,
+template <typename ST, typename R>
+__device__ __forceinline__ void gather(R (&f)[19], const ST* __restrict__ fin, long long NC, int i, int dxm,
                                        int dxp, int dym, int dyp, int dzm, int dzp) {
 #pragma unroll
   for (int q = 0; q < 19; q++) {
     const int cx = CXQ(q), cy = CYQ(q), cz = CZQ(q);
     const int src = i + (cx == 1 ? dxm : (cx == -1 ? dxp : 0)) + (cy == 1 ? dym : (cy == -1 ? dyp : 0)) +
                     (cz == 1 ? dzm : (cz == -1 ? dzp : 0));
-    f[q] = DEV ? Stored<ST>::load_dev(fin + q * NC + src, WQ(q)) : Stored<ST>::load(fin + q * NC + src, WQ(q));
+    f[q] = Stored<ST>::load(fin + q * NC + src, wq<R>(q));
   }
 }
 
@@ -232,138 +273,117 @@ __device__ __forceinline__ void neighbour_deltas(const Geom& g, int x, int y, in
 
 // Boundary rebuild after the gather: the wall plane of the wall axis, then
 // the tangential velocity boundaries in axis order (sim_main.c:383-402).
-template <bool DEV = false>
-__device__ __forceinline__ void boundaries(float (&f)[19], const Geom& g, const FluidParams& p, int x, int y,
-                                           int z) {
+template <typename R>
+__device__ __forceinline__ void boundaries(R (&f)[19], const Geom& g, const FluidParams& p, int x, int y, int z) {
   if (g.wallAxis < 0) return;
   const int c[3] = {x, y, z};
   const int N[3] = {g.Nx, g.Ny, g.Nz};
   const int a = g.wallAxis;
-  if (c[a] == 1) apply_wall<DEV>(f, a, 0, p);
-  else if (c[a] == N[a] - 2) apply_wall<DEV>(f, a, 1, p);
+  if (c[a] == 1) apply_wall(f, a, 0, p);
+  else if (c[a] == N[a] - 2) apply_wall(f, a, 1, p);
 #pragma unroll
   for (int t = 0; t < 3; t++) {
     if (!g.tanBC[t]) continue;
-    if (c[t] == 1) apply_wall<DEV>(f, t, 0, p);
-    else if (c[t] == N[t] - 2) apply_wall<DEV>(f, t, 1, p);
+    if (c[t] == 1) apply_wall(f, t, 0, p);
+    else if (c[t] == N[t] - 2) apply_wall(f, t, 1, p);
   }
 }
 
-// Inverse squared norms of the moment basis rows (rho, e, eps, jx, qx, jy,
-// qy, jz, qz, 3pxx, 3pixx, pww, piww, pxy, pyz, pxz, mx, my, mz).
-#define INV_N1 (1.0f / 2394.0f)
-#define INV_N2 (1.0f / 252.0f)
-#define INV_N4 (1.0f / 40.0f)
-#define INV_N9 (1.0f / 36.0f)
-#define INV_N10 (1.0f / 72.0f)
-#define INV_N11 (1.0f / 12.0f)
-#define INV_N12 (1.0f / 24.0f)
-#define INV_N13 (1.0f / 4.0f)
-#define INV_N16 (1.0f / 8.0f)
-
-// The collision: the reference's MRT with Guo forcing,
-//   f' = f + M^-1 S M n + fg - 0.5 M^-1 S M fg,  n = f_eq - f
-// (GPU_program.cl:396-623), evaluated as one forward and one inverse
-// transform of d = n - fg/2 (linearity):  f' = f + fg + M^T D^-1 S M d.
-// The density row carries no relaxation term (S_rho = 0).  The momentum rows
-// are kept although M_j d = (rho u - j) - g/2 vanishes in exact arithmetic:
-// relaxed with rate 1 they move j onto the first moment of the rounded f_eq
-// every step, as the reference does, instead of letting that rounding
-// difference accumulate as a momentum drift.  COLL 0: the reference's rate
-// vector with 1/tau at rows 8,9,10,14,15 (GPU_program.cl:453, 567-568);
-// COLL 1: BGK.  VISC 0: constant tau; otherwise the local tau of viscosity
-// law VISC (1 Newtonian, 2 power law, 3 Herschel-Bulkley, 4 Casson); -1:
-// both chosen at run time (p.variable, p.viscModel).
-template <int COLL, int VISC>
-__device__ __forceinline__ void collide(float (&f)[19], float rho, float ir, float ux, float uy, float uz, float gx,
-                                        float gy, float gz, float& tau, const FluidParams& p, bool& clamped) {
+template <int COLL, int VISC, typename R>
+__device__ __forceinline__ void collide(R (&f)[19], R rho, R ir, R ux, R uy, R uz, R gx, R gy, R gz, R& tau,
+                                        const FluidParams& p, bool& clamped) {
+  // Inverse squared norms of the moment basis rows (rho, e, eps, jx, qx, jy,
+  // qy, jz, qz, 3pxx, 3pixx, pww, piww, pxy, pyz, pxz, mx, my, mz).
+  const R INV_N1 = R(1) / R(2394), INV_N2 = R(1) / R(252), INV_N3 = R(1) / R(10), INV_N4 = R(1) / R(40);
+  const R INV_N9 = R(1) / R(36), INV_N10 = R(1) / R(72), INV_N11 = R(1) / R(12), INV_N12 = R(1) / R(24);
+  const R INV_N13 = R(1) / R(4), INV_N16 = R(1) / R(8);
   // Equilibrium minus f, pairwise (GPU_program.cl:978-1007), and the Guo term
   // (GPU_program.cl:1010-1038): for a pair +-c the even parts are shared.
-  const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
-  const float uDg = ux * gx + uy * gy + uz * gz;
+  const R usq15 = R(1.5f) * (ux * ux + uy * uy + uz * uz);
+  const R uDg = ux * gx + uy * gy + uz * gz;
   // Correctly rounded rho/3, rho/18, rho/36 as the reference's equilibrium
   // (GPU_program.cl:978-1007): a fluid at rest then has exactly zero
   // non-equilibrium part, which the strain rate of a power-law or yield-
   // stress fluid at rest depends on.
-  const float r0 = rho / 3.0f, r1 = rho / 18.0f, r2 = rho / 36.0f;
-  float d[19], base[19];
+  const R r0 = rho / R(3.0f), r1 = rho / R(18.0f), r2 = rho / R(36.0f);
+  R d[19], base[19];
   {
-    float feq0 = r0 * (1.0f - usq15);
-    float fg0 = -uDg;
-    d[0] = (feq0 - f[0]) - 0.5f * fg0;
+    R feq0 = r0 * (R(1.0f) - usq15);
+    R fg0 = -uDg;
+    d[0] = (feq0 - f[0]) - R(0.5f) * fg0;
     base[0] = f[0] + fg0;
   }
 #define PAIR(qp, qm, cu, cg, rw, gd)                                   \
   {                                                                   \
-    const float cu_ = (cu), cg_ = (cg);                               \
-    const float ev = (rw) * (1.0f + 4.5f * cu_ * cu_ - usq15);        \
-    const float od = (rw) * (3.0f * cu_);                             \
-    const float gev = (-uDg + 3.0f * cu_ * cg_) * (1.0f / (gd));      \
-    const float god = cg_ * (1.0f / (gd));                            \
-    const float fgp = gev + god, fgm = gev - god;                     \
-    d[qp] = ((ev + od) - f[qp]) - 0.5f * fgp;                         \
-    d[qm] = ((ev - od) - f[qm]) - 0.5f * fgm;                         \
+    const R cu_ = (cu), cg_ = (cg);                               \
+    const R ev = (rw) * (R(1.0f) + R(4.5f) * cu_ * cu_ - usq15);        \
+    const R od = (rw) * (R(3.0f) * cu_);                             \
+    const R gev = (-uDg + R(3.0f) * cu_ * cg_) * (R(1.0f) / (gd));      \
+    const R god = cg_ * (R(1.0f) / (gd));                            \
+    const R fgp = gev + god, fgm = gev - god;                     \
+    d[qp] = ((ev + od) - f[qp]) - R(0.5f) * fgp;                         \
+    d[qm] = ((ev - od) - f[qm]) - R(0.5f) * fgm;                         \
     base[qp] = f[qp] + fgp;                                           \
     base[qm] = f[qm] + fgm;                                           \
   }
-  PAIR(1, 2, ux, gx, r1, 6.0f)
-  PAIR(3, 4, uy, gy, r1, 6.0f)
-  PAIR(5, 6, uz, gz, r1, 6.0f)
-  PAIR(7, 12, ux + uy, gx + gy, r2, 12.0f)
-  PAIR(8, 11, ux - uy, gx - gy, r2, 12.0f)
-  PAIR(9, 14, ux + uz, gx + gz, r2, 12.0f)
-  PAIR(10, 13, ux - uz, gx - gz, r2, 12.0f)
-  PAIR(15, 18, uy + uz, gy + gz, r2, 12.0f)
-  PAIR(16, 17, uy - uz, gy - gz, r2, 12.0f)
+  PAIR(1, 2, ux, gx, r1, R(6.0f))
+  PAIR(3, 4, uy, gy, r1, R(6.0f))
+  PAIR(5, 6, uz, gz, r1, R(6.0f))
+  PAIR(7, 12, ux + uy, gx + gy, r2, R(12.0f))
+  PAIR(8, 11, ux - uy, gx - gy, r2, R(12.0f))
+  PAIR(9, 14, ux + uz, gx + gz, r2, R(12.0f))
+  PAIR(10, 13, ux - uz, gx - gz, r2, R(12.0f))
+  PAIR(15, 18, uy + uz, gy + gz, r2, R(12.0f))
+  PAIR(16, 17, uy - uz, gy - gz, r2, R(12.0f))
 #undef PAIR
 
   // Forward transform of d (non-conserved rows only), butterfly form.
-  const float Ax = d[1] + d[2], Bx = d[1] - d[2];
-  const float Ay = d[3] + d[4], By = d[3] - d[4];
-  const float Az = d[5] + d[6], Bz = d[5] - d[6];
-  float Sxy, Xxy, Yxy, Pxy, Sxz, Xxz, Zxz, Pxz, Syz, Yyz, Zyz, Pyz;
+  const R Ax = d[1] + d[2], Bx = d[1] - d[2];
+  const R Ay = d[3] + d[4], By = d[3] - d[4];
+  const R Az = d[5] + d[6], Bz = d[5] - d[6];
+  R Sxy, Xxy, Yxy, Pxy, Sxz, Xxz, Zxz, Pxz, Syz, Yyz, Zyz, Pyz;
   {
-    float a = d[7] + d[8], b = d[11] + d[12], c = d[7] - d[8], e = d[11] - d[12];
+    R a = d[7] + d[8], b = d[11] + d[12], c = d[7] - d[8], e = d[11] - d[12];
     Sxy = a + b; Xxy = a - b; Yxy = c + e; Pxy = c - e;
   }
   {
-    float a = d[9] + d[10], b = d[13] + d[14], c = d[9] - d[10], e = d[13] - d[14];
+    R a = d[9] + d[10], b = d[13] + d[14], c = d[9] - d[10], e = d[13] - d[14];
     Sxz = a + b; Xxz = a - b; Zxz = c + e; Pxz = c - e;
   }
   {
-    float a = d[15] + d[16], b = d[17] + d[18], c = d[15] - d[16], e = d[17] - d[18];
+    R a = d[15] + d[16], b = d[17] + d[18], c = d[15] - d[16], e = d[17] - d[18];
     Syz = a + b; Yyz = a - b; Zyz = c + e; Pyz = c - e;
   }
-  const float A = Ax + Ay + Az, S = Sxy + Sxz + Syz;
-  const float m1 = -30.0f * d[0] - 11.0f * A + 8.0f * S;
-  const float m2 = 12.0f * d[0] - 4.0f * A + S;
-  const float m3 = Bx + Xxy + Xxz;
-  const float m5 = By + Yxy + Yyz;
-  const float m7 = Bz + Zxz + Zyz;
-  const float m4 = -4.0f * Bx + Xxy + Xxz;
-  const float m6 = -4.0f * By + Yxy + Yyz;
-  const float m8 = -4.0f * Bz + Zxz + Zyz;
-  const float T9 = Sxy + Sxz - 2.0f * Syz;
-  const float m9 = 2.0f * Ax - Ay - Az + T9;
-  const float m10 = -4.0f * Ax + 2.0f * Ay + 2.0f * Az + T9;
-  const float T11 = Sxy - Sxz;
-  const float m11 = Ay - Az + T11;
-  const float m12 = -2.0f * Ay + 2.0f * Az + T11;
-  const float m13 = Pxy, m14 = Pyz, m15 = Pxz;
-  const float m16 = Xxy - Xxz, m17 = Yyz - Yxy, m18 = Zxz - Zyz;
+  const R A = Ax + Ay + Az, S = Sxy + Sxz + Syz;
+  const R m1 = -R(30.0f) * d[0] - R(11.0f) * A + R(8.0f) * S;
+  const R m2 = R(12.0f) * d[0] - R(4.0f) * A + S;
+  const R m3 = Bx + Xxy + Xxz;
+  const R m5 = By + Yxy + Yyz;
+  const R m7 = Bz + Zxz + Zyz;
+  const R m4 = -R(4.0f) * Bx + Xxy + Xxz;
+  const R m6 = -R(4.0f) * By + Yxy + Yyz;
+  const R m8 = -R(4.0f) * Bz + Zxz + Zyz;
+  const R T9 = Sxy + Sxz - R(2.0f) * Syz;
+  const R m9 = R(2.0f) * Ax - Ay - Az + T9;
+  const R m10 = -R(4.0f) * Ax + R(2.0f) * Ay + R(2.0f) * Az + T9;
+  const R T11 = Sxy - Sxz;
+  const R m11 = Ay - Az + T11;
+  const R m12 = -R(2.0f) * Ay + R(2.0f) * Az + T11;
+  const R m13 = Pxy, m14 = Pyz, m15 = Pxz;
+  const R m16 = Xxy - Xxz, m17 = Yyz - Yxy, m18 = Zxz - Zyz;
 
   // Rates.
-  float s1, s2, s4, s6, s11, s12, s13, s16;
+  R s1, s2, s4, s6, s11, s12, s13, s16;
   if (COLL == 0) {
-    s1 = 1.19f; s2 = 1.40f; s4 = 1.20f; s6 = 1.20f; s11 = 1.20f; s12 = 1.40f; s13 = 1.40f; s16 = 1.98f;
+    s1 = R(1.19f); s2 = R(1.40f); s4 = R(1.20f); s6 = R(1.20f); s11 = R(1.20f); s12 = R(1.40f); s13 = R(1.40f); s16 = R(1.98f);
   }
 
   if (VISC > 0 || (VISC < 0 && p.variable)) {
     // Strain rate from the relaxed non-equilibrium moments with tau(t-1)
     // (GPU_program.cl:459-562): the second moments of M^-1 S_old M d, which
     // only rows e, 3pxx, pww and the off-diagonal p carry.
-    const float it = __fdividef(1.0f, tau);
-    float a1, a9, a11, a13, a14, a15;
+    const R it = RMath<R>::rcp(tau);
+    R a1, a9, a11, a13, a14, a15;
     if (COLL == 0) {
       a1 = s1 * m1 * INV_N1; a9 = it * m9 * INV_N9; a11 = s11 * m11 * INV_N11;
       a13 = s13 * m13 * INV_N13; a14 = it * m14 * INV_N13; a15 = it * m15 * INV_N13;
@@ -371,25 +391,25 @@ __device__ __forceinline__ void collide(float (&f)[19], float rho, float ir, flo
       a1 = it * m1 * INV_N1; a9 = it * m9 * INV_N9; a11 = it * m11 * INV_N11;
       a13 = it * m13 * INV_N13; a14 = it * m14 * INV_N13; a15 = it * m15 * INV_N13;
     }
-    const float sxx = 42.0f * a1 + 12.0f * a9;
-    const float syy = 42.0f * a1 - 6.0f * a9 + 6.0f * a11;
-    const float szz = 42.0f * a1 - 6.0f * a9 - 6.0f * a11;
-    const float sxy = 4.0f * a13, syz = 4.0f * a14, sxz = 4.0f * a15;
-    const float ss = sxx * sxx + 2.0f * (sxy * sxy + sxz * sxz + syz * syz) + syy * syy + szz * szz;
-    const float srt = sqrtf(ss) * 2.1213203f * ir;
-    tau = compute_tau<VISC>(p, srt, clamped);
+    const R sxx = R(42.0f) * a1 + R(12.0f) * a9;
+    const R syy = R(42.0f) * a1 - R(6.0f) * a9 + R(6.0f) * a11;
+    const R szz = R(42.0f) * a1 - R(6.0f) * a9 - R(6.0f) * a11;
+    const R sxy = R(4.0f) * a13, syz = R(4.0f) * a14, sxz = R(4.0f) * a15;
+    const R ss = sxx * sxx + R(2.0f) * (sxy * sxy + sxz * sxz + syz * syz) + syy * syy + szz * szz;
+    const R srt = RMath<R>::sqrt(ss) * R(2.1213203f) * ir;
+    tau = compute_tau<VISC, R>(p, srt, clamped);
   }
 
-  const float it = __fdividef(1.0f, tau);
-  float a1, a2, a3, a4, a5, a6, a7, a8, a9, a10, a11, a12, a13, a14, a15, a16, a17, a18;
+  const R it = RMath<R>::rcp(tau);
+  R a1, a2, a3, a4, a5, a6, a7, a8, a9, a10, a11, a12, a13, a14, a15, a16, a17, a18;
   if (COLL == 0) {
-    a3 = 0.1f * m3; a5 = 0.1f * m5; a7 = 0.1f * m7;
+    a3 = INV_N3 * m3; a5 = INV_N3 * m5; a7 = INV_N3 * m7;
     a1 = s1 * INV_N1 * m1; a2 = s2 * INV_N2 * m2; a4 = s4 * INV_N4 * m4; a6 = s6 * INV_N4 * m6;
     a8 = it * INV_N4 * m8; a9 = it * INV_N9 * m9; a10 = it * INV_N10 * m10; a11 = s11 * INV_N11 * m11;
     a12 = s12 * INV_N12 * m12; a13 = s13 * INV_N13 * m13; a14 = it * INV_N13 * m14; a15 = it * INV_N13 * m15;
     a16 = s16 * INV_N16 * m16; a17 = s16 * INV_N16 * m17; a18 = s16 * INV_N16 * m18;
   } else {
-    a3 = it * 0.1f * m3; a5 = it * 0.1f * m5; a7 = it * 0.1f * m7;
+    a3 = it * INV_N3 * m3; a5 = it * INV_N3 * m5; a7 = it * INV_N3 * m7;
     a1 = it * INV_N1 * m1; a2 = it * INV_N2 * m2; a4 = it * INV_N4 * m4; a6 = it * INV_N4 * m6;
     a8 = it * INV_N4 * m8; a9 = it * INV_N9 * m9; a10 = it * INV_N10 * m10; a11 = it * INV_N11 * m11;
     a12 = it * INV_N12 * m12; a13 = it * INV_N13 * m13; a14 = it * INV_N13 * m14; a15 = it * INV_N13 * m15;
@@ -397,34 +417,34 @@ __device__ __forceinline__ void collide(float (&f)[19], float rho, float ir, flo
   }
 
   // Inverse transform M^T a, butterfly form.
-  f[0] = base[0] + (-30.0f * a1 + 12.0f * a2);
-  const float bax = -11.0f * a1 - 4.0f * a2;
-  const float Cx = bax + 2.0f * a9 - 4.0f * a10;
-  const float Cy = bax - a9 + 2.0f * a10 + a11 - 2.0f * a12;
-  const float Cz = bax - a9 + 2.0f * a10 - a11 + 2.0f * a12;
-  const float Ox = a3 - 4.0f * a4, Oy = a5 - 4.0f * a6, Oz = a7 - 4.0f * a8;
+  f[0] = base[0] + (-R(30.0f) * a1 + R(12.0f) * a2);
+  const R bax = -R(11.0f) * a1 - R(4.0f) * a2;
+  const R Cx = bax + R(2.0f) * a9 - R(4.0f) * a10;
+  const R Cy = bax - a9 + R(2.0f) * a10 + a11 - R(2.0f) * a12;
+  const R Cz = bax - a9 + R(2.0f) * a10 - a11 + R(2.0f) * a12;
+  const R Ox = a3 - R(4.0f) * a4, Oy = a5 - R(4.0f) * a6, Oz = a7 - R(4.0f) * a8;
   f[1] = base[1] + (Cx + Ox);
   f[2] = base[2] + (Cx - Ox);
   f[3] = base[3] + (Cy + Oy);
   f[4] = base[4] + (Cy - Oy);
   f[5] = base[5] + (Cz + Oz);
   f[6] = base[6] + (Cz - Oz);
-  const float bd = 8.0f * a1 + a2;
+  const R bd = R(8.0f) * a1 + a2;
   {  // xy: 7 (+,+) 8 (+,-) 11 (-,+) 12 (-,-)
-    const float E = bd + a9 + a10 + a11 + a12, X = a3 + a4 + a16, Y = a5 + a6 - a17, P = a13;
-    const float u1 = E + P, u2 = E - P, v1 = X + Y, v2 = X - Y;
+    const R E = bd + a9 + a10 + a11 + a12, X = a3 + a4 + a16, Y = a5 + a6 - a17, P = a13;
+    const R u1 = E + P, u2 = E - P, v1 = X + Y, v2 = X - Y;
     f[7] = base[7] + (u1 + v1); f[12] = base[12] + (u1 - v1);
     f[8] = base[8] + (u2 + v2); f[11] = base[11] + (u2 - v2);
   }
   {  // xz: 9 (+,+) 10 (+,-) 13 (-,+) 14 (-,-)
-    const float E = bd + a9 + a10 - a11 - a12, X = a3 + a4 - a16, Z = a7 + a8 + a18, P = a15;
-    const float u1 = E + P, u2 = E - P, v1 = X + Z, v2 = X - Z;
+    const R E = bd + a9 + a10 - a11 - a12, X = a3 + a4 - a16, Z = a7 + a8 + a18, P = a15;
+    const R u1 = E + P, u2 = E - P, v1 = X + Z, v2 = X - Z;
     f[9] = base[9] + (u1 + v1); f[14] = base[14] + (u1 - v1);
     f[10] = base[10] + (u2 + v2); f[13] = base[13] + (u2 - v2);
   }
   {  // yz: 15 (+,+) 16 (+,-) 17 (-,+) 18 (-,-)
-    const float E = bd - 2.0f * a9 - 2.0f * a10, Y = a5 + a6 + a17, Z = a7 + a8 - a18, P = a14;
-    const float u1 = E + P, u2 = E - P, v1 = Y + Z, v2 = Y - Z;
+    const R E = bd - R(2.0f) * a9 - R(2.0f) * a10, Y = a5 + a6 + a17, Z = a7 + a8 - a18, P = a14;
+    const R u1 = E + P, u2 = E - P, v1 = Y + Z, v2 = Y - Z;
     f[15] = base[15] + (u1 + v1); f[18] = base[18] + (u1 - v1);
     f[16] = base[16] + (u2 + v2); f[17] = base[17] + (u2 - v2);
   }
@@ -440,8 +460,15 @@ struct __align__(16) SpreadSmem {
   union {
     unsigned long long acc[3][HALO_N];  // fixed-point sums: lo parts (low word), hi parts (high word)
     float g[3][HALO_N];                 // the spread force of the halo nodes
+    double g64[3][HALO_N];              // the same in the FP64 build
   };
 };
+template <typename R>
+__device__ __forceinline__ R* halo_field(SpreadSmem& s);
+template <>
+__device__ __forceinline__ float* halo_field<float>(SpreadSmem& s) { return &s.g[0][0]; }
+template <>
+__device__ __forceinline__ double* halo_field<double>(SpreadSmem& s) { return &s.g64[0][0]; }
 static_assert((3 * HALO_N) % 2 == 0, "the sums are cleared sixteen bytes at a time");
 constexpr int SPREAD_CONVERT_PER_THREAD = (3 * HALO_N + FLUID_THREADS - 1) / FLUID_THREADS;
 
@@ -483,6 +510,7 @@ __device__ __forceinline__ int fixed_exponent(unsigned fmax_bits) {
 // the two parts are summed exactly with 32-bit atomics, lo in the low word and
 // hi in the high word of the node's 64-bit slot; each sum is converted back
 // with one rounding.  Needs all FLUID_THREADS threads.
+template <typename R = float>
 __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& tl, long long T, int n, int X0,
                                 int Y0, int Z0, int tid, int k, int first_id, unsigned* err) {
   float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
@@ -534,24 +562,27 @@ __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& t
   }
   __syncthreads();
   // value = (hi * 2^16 + lo) * 2^-k, both parts scaled exactly by powers of
-  // two and joined with one rounding.  All sums are read before the float
-  // field overwrites them.
-  const float inv = ldexpf(1.0f, -k), inv_hi = ldexpf(1.0f, 16 - k);
-  float v[SPREAD_CONVERT_PER_THREAD];
+  // two and joined with one rounding (exactly in FP64).  All sums are read
+  // before the field overwrites them.
+  R v[SPREAD_CONVERT_PER_THREAD];
 #pragma unroll
   for (int r = 0; r < SPREAD_CONVERT_PER_THREAD; r++) {
     const int h = tid + r * FLUID_THREADS;
-    v[r] = 0.0f;
+    v[r] = R(0);
     if (h < 3 * HALO_N) {
       const unsigned* slot = reinterpret_cast<const unsigned*>(&(&s.acc[0][0])[h]);
-      v[r] = __fmaf_rn((float)(int)slot[1], inv_hi, (float)slot[0] * inv);
+      if (sizeof(R) == 4)
+        v[r] = __fmaf_rn((float)(int)slot[1], ldexpf(1.0f, 16 - k), (float)slot[0] * ldexpf(1.0f, -k));
+      else
+        v[r] = (R)(ldexp((double)(int)slot[1], 16 - k) + ldexp((double)slot[0], -k));
     }
   }
   __syncthreads();
+  R* field = halo_field<R>(s);
 #pragma unroll
   for (int r = 0; r < SPREAD_CONVERT_PER_THREAD; r++) {
     const int h = tid + r * FLUID_THREADS;
-    if (h < 3 * HALO_N) (&s.g[0][0])[h] = v[r];
+    if (h < 3 * HALO_N) field[h] = v[r];
   }
   __syncthreads();
 }
@@ -560,23 +591,25 @@ __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& t
 // 27-point stencil (weights 1/4, 1/2, 1/4 per axis; GPU_program.cl:356-377)
 // over the halo field s.g.  Each thread takes two consecutive z-planes, so the
 // 9-point x-y sums of the two middle halo planes are shared between its nodes.
-__device__ __forceinline__ void smooth_pair(const SpreadSmem& s, int tx, int ty, int tz, float (&sg)[2][3]) {
+template <typename R>
+__device__ __forceinline__ void smooth_pair(SpreadSmem& s, int tx, int ty, int tz, R (&sg)[2][3]) {
   const int hx = tx + 1, hy = ty + 1, hz0 = 2 * tz;
+  const R* gf = halo_field<R>(s);
 #pragma unroll
   for (int pl = 0; pl < 4; pl++) {
-    float px = 0.0f, py = 0.0f, pz = 0.0f;
+    R px = R(0), py = R(0), pz = R(0);
 #pragma unroll
     for (int sy = -1; sy <= 1; sy++)
 #pragma unroll
       for (int sx = -1; sx <= 1; sx++) {
-        const float ws = (sx == 0 ? 0.5f : 0.25f) * (sy == 0 ? 0.5f : 0.25f);
+        const R ws = R(sx == 0 ? 0.5f : 0.25f) * R(sy == 0 ? 0.5f : 0.25f);
         const int h = (hx + sx) + HALO_X * ((hy + sy) + HALO_Y * (hz0 + pl));
-        px += ws * s.g[0][h];
-        py += ws * s.g[1][h];
-        pz += ws * s.g[2][h];
+        px += ws * gf[h];
+        py += ws * gf[HALO_N + h];
+        pz += ws * gf[2 * HALO_N + h];
       }
-    const float w0 = pl == 0 ? 0.25f : (pl == 1 ? 0.5f : (pl == 2 ? 0.25f : 0.0f));
-    const float w1 = pl == 0 ? 0.0f : (pl == 1 ? 0.25f : (pl == 2 ? 0.5f : 0.25f));
+    const R w0 = R(pl == 0 ? 0.25f : (pl == 1 ? 0.5f : (pl == 2 ? 0.25f : 0.0f)));
+    const R w1 = R(pl == 0 ? 0.0f : (pl == 1 ? 0.25f : (pl == 2 ? 0.5f : 0.25f)));
     if (pl < 3) {
       sg[0][0] += w0 * px; sg[0][1] += w0 * py; sg[0][2] += w0 * pz;
     }
@@ -622,11 +655,13 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
   const int y = Y0 + threadIdx.y;
   const long long NC = g.NC;
   const bool inxy = x >= 1 && x <= g.Nx - 2 && y >= 1 && y <= g.Ny - 2;
+  using R = typename RealOf<ST>::type;
+  constexpr bool k64 = sizeof(R) == 8;
 
   // IBM force of the tile: the markers listed by the particle pass of step
   // t-1, accumulated over the tile's halo and smoothed with the reference's
   // 27-point stencil (GPU_program.cl:356-377), in shared memory only.
-  float sg[2][3] = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}};
+  R sg[2][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
   if (a.has_ibm) {
     const int cnt = a.tiles.count[T];
     const int first_id = tid < a.tiles.cap ? a.tiles.list[(long long)T * a.tiles.cap + tid] : 0;  // speculative
@@ -639,8 +674,8 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
       if (T == 0) a.tiles.fmax[a.t & 1] = 0u;
     }
     if (cnt > 0) {
-      accumulate_tile(sm, g, a.tiles, T, min(cnt, a.tiles.cap), X0, Y0, Z0, tid, fixed_exponent(fbits), first_id,
-                      a.err);
+      accumulate_tile<R>(sm, g, a.tiles, T, min(cnt, a.tiles.cap), X0, Y0, Z0, tid, fixed_exponent(fbits), first_id,
+                         a.err);
       smooth_pair(sm, threadIdx.x, threadIdx.y, threadIdx.z, sg);
     }
   }
@@ -651,10 +686,10 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
     const int z = Z0 + 2 * threadIdx.z + zz;
     if (!inxy || z < 1 || z > g.Nz - 2) continue;
     const int i = x + g.Nx * (y + g.Ny * z);
-    float f[19];
+    R f[19];
     if (first) {
 #pragma unroll
-      for (int q = 0; q < 19; q++) f[q] = Stored<ST>::load(fin + q * NC + i, WQ(q));
+      for (int q = 0; q < 19; q++) f[q] = Stored<ST>::load(fin + q * NC + i, wq<R>(q));
     } else if (BC == BC_ZWALL) {
       const int Nxy = g.Nx * g.Ny;
       const int dxm = x == 1 ? g.Nx - 3 : -1;
@@ -670,38 +705,43 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
       gather(f, fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp);
       boundaries(f, g, a.p, x, y, z);
     }
-    const float gx = a.p.g[0] + (zz ? sg[1][0] : sg[0][0]);
-    const float gy = a.p.g[1] + (zz ? sg[1][1] : sg[0][1]);
-    const float gz = a.p.g[2] + (zz ? sg[1][2] : sg[0][2]);
-    float rho = 0.0f;
+    const R gx = R(a.p.g[0]) + (zz ? sg[1][0] : sg[0][0]);
+    const R gy = R(a.p.g[1]) + (zz ? sg[1][1] : sg[0][1]);
+    const R gz = R(a.p.g[2]) + (zz ? sg[1][2] : sg[0][2]);
+    R rho = R(0);
 #pragma unroll
     for (int q = 0; q < 19; q++) rho += f[q];
-    const float jx = f[1] - f[2] + f[7] + f[8] + f[9] + f[10] - f[11] - f[12] - f[13] - f[14];
-    const float jy = f[3] - f[4] + f[7] - f[8] + f[11] - f[12] + f[15] + f[16] - f[17] - f[18];
-    const float jz = f[5] - f[6] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16] + f[17] - f[18];
-    const float ir = __fdividef(1.0f, rho);
-    const float ux = (jx + 0.5f * gx) * ir, uy = (jy + 0.5f * gy) * ir, uz = (jz + 0.5f * gz) * ir;
-    a.u[i] = ux;
-    a.u[i + NC] = uy;
-    a.u[i + 2 * NC] = uz;
+    const R jx = f[1] - f[2] + f[7] + f[8] + f[9] + f[10] - f[11] - f[12] - f[13] - f[14];
+    const R jy = f[3] - f[4] + f[7] - f[8] + f[11] - f[12] + f[15] + f[16] - f[17] - f[18];
+    const R jz = f[5] - f[6] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16] + f[17] - f[18];
+    const R ir = RMath<R>::rcp(rho);
+    const R ux = (jx + R(0.5f) * gx) * ir, uy = (jy + R(0.5f) * gy) * ir, uz = (jz + R(0.5f) * gz) * ir;
+    a.u[i] = (float)ux;
+    a.u[i + NC] = (float)uy;
+    a.u[i + 2 * NC] = (float)uz;
     // A non-finite population makes rho non-finite; a vanishing or negative
     // density is flagged too.
-    if (!(rho > 0.0f && rho < 1e30f)) atomicOr(a.err, ERR_NONFINITE);
-    float tau = var ? a.tau[i] : a.p.tauN;
+    if (!(rho > R(0) && rho < R(1e30f))) atomicOr(a.err, ERR_NONFINITE);
+    // The FP64 build keeps tau in double (tau64) and a float copy for
+    // read-back.
+    R tau = var ? (k64 ? R(a.tau64[i]) : R(a.tau[i])) : R(a.p.tauN);
     bool clamped = false;
-    collide<COLL, VISC>(f, rho, ir, ux, uy, uz, gx, gy, gz, tau, a.p, clamped);
+    collide<COLL, VISC, R>(f, rho, ir, ux, uy, uz, gx, gy, gz, tau, a.p, clamped);
     if (var) {
-      a.tau[i] = tau;
+      if (k64) a.tau64[i] = (double)tau;
+      a.tau[i] = (float)tau;
       nclamp += clamped ? 1 : 0;
     }
 #pragma unroll
-    for (int q = 0; q < 19; q++) Stored<ST>::store(fout + q * NC + i, f[q], WQ(q));
+    for (int q = 0; q < 19; q++) Stored<ST>::store(fout + q * NC + i, f[q], wq<R>(q));
   }
   if (var && nclamp) atomicAdd(a.clamps, (unsigned long long)nclamp);
 }
 
 template <int COLL, int VISC, int BC, typename ST>
-__global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? FLUID_MIN_BLOCKS_F32 : FLUID_MIN_BLOCKS)
+__global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4   ? FLUID_MIN_BLOCKS_F32
+                                                 : sizeof(ST) == 8 ? 2
+                                                                   : FLUID_MIN_BLOCKS)
     fluid_step_kernel(const FluidArgs a, const int first) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   fluid_tile<COLL, VISC, BC, ST>(a, first, blockIdx.x, blockIdx.y, blockIdx.z,
@@ -745,11 +785,11 @@ __global__ void materialize_f_kernel(const FluidArgs a, float* __restrict__ out)
     const int i = x + g.Nx * (y + g.Ny * z);
     int dxm, dxp, dym, dyp, dzm, dzp;
     neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
-    float f[19];
+    typename RealOf<ST>::type f[19];
     gather(f, static_cast<const ST*>(a.fin), NC, i, dxm, dxp, dym, dyp, dzm, dzp);
     boundaries(f, g, a.p, x, y, z);
 #pragma unroll
-    for (int q = 0; q < 19; q++) out[q * NC + i] = f[q];
+    for (int q = 0; q < 19; q++) out[q * NC + i] = (float)f[q];
   }
 }
 
@@ -922,6 +962,72 @@ __device__ bool pair_force(const ParticleParams& P, const Kin& A, const Kin& B, 
   return any;
 }
 
+// Lists marker gid in every fluid tile whose halo holds one of its stencil
+// nodes (up to 2 tiles per axis, 3 where the stencil wraps a periodic edge
+// of a lattice whose N-2 is a multiple of the tile size); lanes inserting
+// into the same tile share one atomic.  Up to 8 atomics of the warp are
+// issued before any result is used, so their round trips overlap.  All 32
+// lanes of the warp call it (n = 0 for lanes without a marker).
+__device__ __forceinline__ void insert_marker(const ParticleArgs& a, long long gid, int lane, const int (&tx)[4],
+                                              const int (&ty)[4], const int (&tz)[4], int nx, int ny, int nz) {
+  const Geom& g = a.g;
+  const int n = nx * ny * nz;
+  int nmax = n;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+  // Entry j of the marker's tile product, j = ia + nx*(ib + ny*ic), advanced
+  // incrementally (no divisions).
+  int ia = 0, ib = 0, ic = 0;
+  for (int j0 = 0; j0 < nmax; j0 += 8) {
+    int tileOf[8], baseOf[8];
+    unsigned peersOf[8];
+#pragma unroll
+    for (int jj = 0; jj < 8; jj++) {
+      const int j = j0 + jj;
+      tileOf[jj] = -1;
+      baseOf[jj] = 0;
+      peersOf[jj] = 0u;
+      if (j >= nmax) continue;
+      const bool act = j < n;
+      const unsigned amask = __ballot_sync(0xffffffffu, act);
+      if (act) {
+        const int T = tx[ia] + g.ntx * (ty[ib] + g.nty * tz[ic]);
+        const unsigned peers = __match_any_sync(amask, T);
+        tileOf[jj] = T;
+        peersOf[jj] = peers;
+        if (lane == __ffs(peers) - 1) baseOf[jj] = atomicAdd(&a.tiles.count[T], __popc(peers));
+        if (++ia == nx) {
+          ia = 0;
+          if (++ib == ny) {
+            ib = 0;
+            ++ic;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int jj = 0; jj < 8; jj++) {
+      if (j0 + jj >= nmax) continue;
+      const int base = __shfl_sync(0xffffffffu, baseOf[jj], peersOf[jj] ? __ffs(peersOf[jj]) - 1 : lane);
+      if (tileOf[jj] >= 0) {
+        const int slot = base + __popc(peersOf[jj] & ((1u << lane) - 1u));
+        if (slot < a.tiles.cap) a.tiles.list[(long long)tileOf[jj] * a.tiles.cap + slot] = (int)gid;
+        else atomicOr(a.err, ERR_TILE_OVERFLOW);
+      }
+    }
+  }
+}
+
+// Largest force component of the step (the fixed-point unit of the spread):
+// warp maximum, then one atomic per warp.  All 32 lanes call it.
+__device__ __forceinline__ void record_fmax(const ParticleArgs& a, float fx, float fy, float fz, int lane) {
+  float fm = fmaxf(fabsf(fx), fmaxf(fabsf(fy), fabsf(fz)));
+  if (!(fm == fm)) fm = 3.0e38f;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) fm = fmaxf(fm, __shfl_xor_sync(0xffffffffu, fm, o));
+  if (lane == 0 && fm > 0.0f) atomicMax(&a.tiles.fmax[a.t & 1], __float_as_uint(fm));
+}
+
 // One reference work-group of markers (group grp of np*nfa) per block:
 // red holds 2*blockDim.x float4 (forces, then torques), s_kin the sphere's
 // updated state.
@@ -995,66 +1101,9 @@ __device__ __forceinline__ void particle_group(const ParticleArgs& a, const int 
       }
     }
     // List the marker in every fluid tile whose halo holds one of its
-    // stencil nodes (up to 2 tiles per axis, 3 where the stencil wraps a
-    // periodic edge); lanes inserting into the same tile share one atomic.
-    // Up to 8 atomics of the warp are issued before any result is used, so
-    // their round trips overlap.
-    {
-      const int n = nx * ny * nz;
-      int nmax = n;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
-      // Entry j of the marker's tile product, j = ia + nx*(ib + ny*ic),
-      // advanced incrementally (no divisions).
-      int ia = 0, ib = 0, ic = 0;
-      for (int j0 = 0; j0 < nmax; j0 += 8) {
-        int tileOf[8], baseOf[8];
-        unsigned peersOf[8];
-#pragma unroll
-        for (int jj = 0; jj < 8; jj++) {
-          const int j = j0 + jj;
-          tileOf[jj] = -1;
-          baseOf[jj] = 0;
-          peersOf[jj] = 0u;
-          if (j >= nmax) continue;
-          const bool act = j < n;
-          const unsigned amask = __ballot_sync(0xffffffffu, act);
-          if (act) {
-            const int T = tx[ia] + g.ntx * (ty[ib] + g.nty * tz[ic]);
-            const unsigned peers = __match_any_sync(amask, T);
-            tileOf[jj] = T;
-            peersOf[jj] = peers;
-            if (lane == __ffs(peers) - 1) baseOf[jj] = atomicAdd(&a.tiles.count[T], __popc(peers));
-            if (++ia == nx) {
-              ia = 0;
-              if (++ib == ny) {
-                ib = 0;
-                ++ic;
-              }
-            }
-          }
-        }
-#pragma unroll
-        for (int jj = 0; jj < 8; jj++) {
-          if (j0 + jj >= nmax) continue;
-          const int base = __shfl_sync(0xffffffffu, baseOf[jj], peersOf[jj] ? __ffs(peersOf[jj]) - 1 : lane);
-          if (tileOf[jj] >= 0) {
-            const int slot = base + __popc(peersOf[jj] & ((1u << lane) - 1u));
-            if (slot < a.tiles.cap) a.tiles.list[(long long)tileOf[jj] * a.tiles.cap + slot] = (int)gid;
-            else atomicOr(a.err, ERR_TILE_OVERFLOW);
-          }
-        }
-      }
-    }
-    // Largest force component of the step (fixed-point unit of the spread):
-    // warp maximum, then one atomic per warp.
-    {
-      float fm = fmaxf(fabsf(force.x), fmaxf(fabsf(force.y), fabsf(force.z)));
-      if (!(fm == fm)) fm = 3.0e38f;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) fm = fmaxf(fm, __shfl_xor_sync(0xffffffffu, fm, o));
-      if (lane == 0 && fm > 0.0f) atomicMax(&a.tiles.fmax[a.t & 1], __float_as_uint(fm));
-    }
+    // stencil nodes; record the step's largest force component.
+    insert_marker(a, gid, lane, tx, ty, tz, nx, ny, nz);
+    record_fmax(a, force.x, force.y, force.z, lane);
     // Work-group reduction in the reference's tree order
     // (GPU_program.cl:232-255).
     const int B = blockDim.x;
@@ -1073,6 +1122,178 @@ __device__ __forceinline__ void particle_group(const ParticleArgs& a, const int 
       a.pff_new[grp + ngroups] = red[B];
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// The FP64 particle pass (particle_precision = 1): the same steps as
+// particle_group, with the sphere state, the per-sphere force and torque sums
+// and the Newton-Euler integration in double.  The fluid-side records (marker
+// weights and forces, read-back copies of the state and partials) are float.
+struct Kin64 {
+  double4 x, v, q, w;
+};
+
+__device__ __forceinline__ double4 d4(const double* p) { return make_double4(p[0], p[1], p[2], p[3]); }
+__device__ __forceinline__ void d4st(double* p, double4 v) {
+  p[0] = v.x;
+  p[1] = v.y;
+  p[2] = v.z;
+  p[3] = v.w;
+}
+__device__ __forceinline__ double4 d4add(double4 a, double4 b) {
+  return make_double4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ double4 d4mul(double4 a, double s) { return make_double4(a.x * s, a.y * s, a.z * s, a.w * s); }
+__device__ __forceinline__ double4 d4cross(double4 a, double4 b) {
+  return make_double4(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x, 0.0);
+}
+__device__ __forceinline__ double4 f2d(float4 a) { return make_double4(a.x, a.y, a.z, a.w); }
+__device__ __forceinline__ float4 d2f(double4 a) {
+  return make_float4((float)a.x, (float)a.y, (float)a.z, (float)a.w);
+}
+__device__ __forceinline__ double wrap_mod64(double a, double w) {
+  if (a >= 0.0 && a < w) return a;
+  if (a >= w && a < 2.0 * w) return a - w;
+  return fmod(a, w);
+}
+
+// particle_dynamics (CPU_program.cl:209-276) in double.
+__device__ Kin64 rigid_update_f64(const ParticleArgs& a, int p) {
+  const ParticleParams& P = a.p;
+  const int np = P.np, nfa = P.nfa;
+  Kin64 k;
+  k.x = d4(a.kin64_old + 4 * (size_t)p);
+  k.v = d4(a.kin64_old + 4 * (size_t)(p + np));
+  k.q = d4(a.kin64_old + 4 * (size_t)(p + 2 * np));
+  k.w = d4(a.kin64_old + 4 * (size_t)(p + 3 * np));
+  if (P.fixed) return k;
+  double4 acc = make_double4(0, 0, 0, 0), aacc = acc;
+  for (int fa = 0; fa < nfa; fa++) {
+    acc = d4add(acc, d4(a.pff64_old + 4 * (size_t)(p * nfa + fa)));
+    aacc = d4add(aacc, d4(a.pff64_old + 4 * (size_t)((p + np) * nfa + fa)));
+  }
+  acc = d4add(acc, f2d(a.pf_old[p]));
+  aacc = d4add(aacc, f2d(a.pf_old[p + np]));
+  acc = d4mul(acc, 1.0 / (double)P.mass);
+  aacc = d4mul(aacc, 1.0 / (double)P.inertia);
+  acc.x += P.g[0];
+  acc.y += P.g[1];
+  acc.z += P.g[2];
+  const double4 W = make_double4(P.S[0], P.S[1], P.S[2], 1.0);
+  const double4 rw = d4add(d4add(d4add(k.x, k.v), d4mul(acc, 0.5)), W);
+  Kin64 o;
+  o.x = make_double4(wrap_mod64(rw.x, W.x), wrap_mod64(rw.y, W.y), wrap_mod64(rw.z, W.z), wrap_mod64(rw.w, W.w));
+  o.v = d4add(k.v, acc);
+  const double dqw = -(k.w.x * k.q.x + k.w.y * k.q.y + k.w.z * k.q.z + k.w.w * k.q.w);
+  const double4 dq = d4add(d4mul(k.w, k.q.w), d4cross(k.w, k.q));
+  o.q = d4mul(dq, 0.5);
+  o.q.w += 0.5 * dqw;
+  o.w = d4add(k.w, aacc);
+  return o;
+}
+
+// One work-group of markers, FP64 state and sums; red holds 2*blockDim.x
+// double4 (forces, then torques), summed in the reference's tree order.
+__device__ __forceinline__ void particle_group_f64(const ParticleArgs& a, const int grp, double4* red, Kin64& s_kin) {
+  const ParticleParams& P = a.p;
+  const Geom& g = a.g;
+  const int np = P.np, nfa = P.nfa, L = P.L;
+  const int ngroups = np * nfa;
+  const int l = threadIdx.x;
+  const int lane = l & 31;
+  const int p = grp / nfa;
+  const int wg = grp - p * nfa;
+  const float4 r0f = l < L ? a.sphere[wg * L + l] : make_float4(0.f, 0.f, 0.f, 0.f);
+  if (l == 0) {
+    const Kin64 kn = rigid_update_f64(a, p);
+    s_kin = kn;
+    if (wg == 0) {
+      d4st(a.kin64_new + 4 * (size_t)p, kn.x);
+      d4st(a.kin64_new + 4 * (size_t)(p + np), kn.v);
+      d4st(a.kin64_new + 4 * (size_t)(p + 2 * np), kn.q);
+      d4st(a.kin64_new + 4 * (size_t)(p + 3 * np), kn.w);
+      a.kin_new[p] = d2f(kn.x);
+      a.kin_new[p + np] = d2f(kn.v);
+      a.kin_new[p + 2 * np] = d2f(kn.q);
+      a.kin_new[p + 3 * np] = d2f(kn.w);
+    }
+  }
+  __syncthreads();
+  const Kin64 k = s_kin;
+  double4 force = make_double4(0, 0, 0, 0), torque = force;
+  int tx[4], ty[4], tz[4], nx = 0, ny = 0, nz = 0;
+  const long long gid = (long long)grp * L + l;
+  if (l < L) {
+    const double4 r0 = f2d(r0f);
+    const double4 W = make_double4(P.S[0], P.S[1], P.S[2], 1.0);
+    const double4 rw = d4add(d4add(k.x, r0), W);
+    const double4 rpp =
+        make_double4(wrap_mod64(rw.x, W.x), wrap_mod64(rw.y, W.y), wrap_mod64(rw.z, W.z), wrap_mod64(rw.w, W.w));
+    const double fx = floor(rpp.x), fy = floor(rpp.y), fz = floor(rpp.z);
+    const int x0 = (int)fx + P.buffer[0], y0 = (int)fy + P.buffer[1], z0 = (int)fz + P.buffer[2];
+    const bool ok = fx == fx && fy == fy && fz == fz && x0 >= 1 && x0 <= g.Nx - 2 && y0 >= 1 && y0 <= g.Ny - 2 &&
+                    z0 >= 1 && z0 <= g.Nz - 2;
+    if (!ok) {
+      atomicOr(a.err, ERR_NONFINITE);
+    } else {
+      const int xs = (x0 == g.Nx - 2) ? -(g.Nx - 3) : 1;
+      const int ys = (y0 == g.Ny - 2) ? -(g.Ny - 3) : 1;
+      const int zs = (z0 == g.Nz - 2) ? -(g.Nz - 3) : 1;
+      const double wx = 1.0 - (rpp.x - fx), wy = 1.0 - (rpp.y - fy), wz = 1.0 - (rpp.z - fz);
+      const double w[8] = {wx * wy * wz,
+                           (1.0 - wx) * wy * wz,
+                           wx * (1.0 - wy) * wz,
+                           wx * wy * (1.0 - wz),
+                           (1.0 - wx) * (1.0 - wy) * wz,
+                           (1.0 - wx) * wy * (1.0 - wz),
+                           wx * (1.0 - wy) * (1.0 - wz),
+                           (1.0 - wx) * (1.0 - wy) * (1.0 - wz)};
+      const int sh[8][3] = {{0, 0, 0}, {xs, 0, 0}, {0, ys, 0}, {0, 0, zs}, {xs, ys, 0}, {xs, 0, zs},
+                            {0, ys, zs}, {xs, ys, zs}};
+      double ux = 0.0, uy = 0.0, uz = 0.0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const long long i =
+            (x0 + sh[j][0]) + (long long)g.Nx * ((y0 + sh[j][1]) + (long long)g.Ny * (z0 + sh[j][2]));
+        ux += w[j] * a.u[i];
+        uy += w[j] * a.u[i + g.NC];
+        uz += w[j] * a.u[i + 2 * g.NC];
+      }
+      const double4 vpp = d4add(k.v, d4cross(k.w, r0));
+      force = d4mul(make_double4(ux - vpp.x, uy - vpp.y, uz - vpp.z, -vpp.w), (double)P.pointArea);
+      torque = d4cross(r0, force);
+      a.mrec[2 * gid] = make_float4((float)wx, (float)wy, (float)wz, __uint_as_float((unsigned)x0 | ((unsigned)y0 << 16)));
+      a.mrec[2 * gid + 1] = make_float4((float)force.x, (float)force.y, (float)force.z, __uint_as_float((unsigned)z0));
+      nx = tile_set(x0, x0 + xs, TILE_X, g.ntx, tx);
+      ny = tile_set(y0, y0 + ys, TILE_Y, g.nty, ty);
+      nz = tile_set(z0, z0 + zs, TILE_Z, g.ntz, tz);
+    }
+  }
+  insert_marker(a, gid, lane, tx, ty, tz, nx, ny, nz);
+  record_fmax(a, (float)force.x, (float)force.y, (float)force.z, lane);
+  const int B = blockDim.x;
+  red[l] = force;
+  red[l + B] = torque;
+  __syncthreads();
+  for (int s = L / 2; s > 0; s >>= 1) {
+    if (l < s) {
+      red[l] = d4add(red[l], red[l + s]);
+      red[l + B] = d4add(red[l + B], red[l + s + B]);
+    }
+    __syncthreads();
+  }
+  if (l == 0) {
+    d4st(a.pff64_new + 4 * (size_t)grp, red[0]);
+    d4st(a.pff64_new + 4 * (size_t)(grp + ngroups), red[B]);
+    a.pff_new[grp] = d2f(red[0]);
+    a.pff_new[grp + ngroups] = d2f(red[B]);
+  }
+}
+
+__global__ void particle_step_f64_kernel(const ParticleArgs a) {
+  extern __shared__ double4 red64[];
+  __shared__ Kin64 s_kin;
+  particle_group_f64(a, blockIdx.x, red64, s_kin);
 }
 
 __global__ void particle_step_kernel(const ParticleArgs a) {
@@ -1381,20 +1602,30 @@ static cudaError_t launch_fluid_st(const FluidArgs& a, bool first, bool variable
 }
 
 cudaError_t launch_fluid(const FluidArgs& a, bool first, bool variable, int collision, int storage, cudaStream_t s) {
+  if (storage == STORE_F64) {
+    // The FP64 build: the reference's MRT only.
+    if (collision != 0) return cudaErrorInvalidValue;
+    const Geom& g = a.g;
+    const bool zwall = g.periodic[0] && g.periodic[1] && g.wallAxis == 2 && !g.tanBC[0] && !g.tanBC[1] && !g.tanBC[2];
+    return zwall ? launch_fluid_v<0, BC_ZWALL, double>(a, first, variable, s)
+                 : launch_fluid_v<0, BC_GENERIC, double>(a, first, variable, s);
+  }
   if (storage == STORE_F16) return launch_fluid_st<__half>(a, first, variable, collision, s);
   if (storage == STORE_BF16) return launch_fluid_st<__nv_bfloat16>(a, first, variable, collision, s);
   return launch_fluid_st<float>(a, first, variable, collision, s);
 }
 
 cudaError_t launch_materialize_f(const FluidArgs& a, int storage, float* out, cudaStream_t s) {
-  if (storage == STORE_F16) materialize_f_kernel<__half><<<1184, 256, 0, s>>>(a, out);
+  if (storage == STORE_F64) materialize_f_kernel<double><<<1184, 256, 0, s>>>(a, out);
+  else if (storage == STORE_F16) materialize_f_kernel<__half><<<1184, 256, 0, s>>>(a, out);
   else if (storage == STORE_BF16) materialize_f_kernel<__nv_bfloat16><<<1184, 256, 0, s>>>(a, out);
   else materialize_f_kernel<float><<<1184, 256, 0, s>>>(a, out);
   return cudaGetLastError();
 }
 
 cudaError_t launch_store_f(const float* in, void* out, long long NC, int storage, cudaStream_t s) {
-  if (storage == STORE_F16) store_f_kernel<__half><<<1184, 256, 0, s>>>(in, static_cast<__half*>(out), NC);
+  if (storage == STORE_F64) store_f_kernel<double><<<1184, 256, 0, s>>>(in, static_cast<double*>(out), NC);
+  else if (storage == STORE_F16) store_f_kernel<__half><<<1184, 256, 0, s>>>(in, static_cast<__half*>(out), NC);
   else if (storage == STORE_BF16)
     store_f_kernel<__nv_bfloat16><<<1184, 256, 0, s>>>(in, static_cast<__nv_bfloat16*>(out), NC);
   else store_f_kernel<float><<<1184, 256, 0, s>>>(in, static_cast<float*>(out), NC);
@@ -1402,7 +1633,8 @@ cudaError_t launch_store_f(const float* in, void* out, long long NC, int storage
 }
 
 cudaError_t launch_load_f(const void* in, float* out, long long NC, int storage, cudaStream_t s) {
-  if (storage == STORE_F16) load_f_kernel<__half><<<1184, 256, 0, s>>>(static_cast<const __half*>(in), out, NC);
+  if (storage == STORE_F64) load_f_kernel<double><<<1184, 256, 0, s>>>(static_cast<const double*>(in), out, NC);
+  else if (storage == STORE_F16) load_f_kernel<__half><<<1184, 256, 0, s>>>(static_cast<const __half*>(in), out, NC);
   else if (storage == STORE_BF16)
     load_f_kernel<__nv_bfloat16><<<1184, 256, 0, s>>>(static_cast<const __nv_bfloat16*>(in), out, NC);
   else load_f_kernel<float><<<1184, 256, 0, s>>>(static_cast<const float*>(in), out, NC);
@@ -1412,6 +1644,10 @@ cudaError_t launch_load_f(const void* in, float* out, long long NC, int storage,
 cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s) {
   const int ngroups = a.p.np * a.p.nfa;
   const int threads = a.p.L < 128 ? 128 : a.p.L;
+  if (a.p64) {
+    particle_step_f64_kernel<<<ngroups, threads, sizeof(double4) * 2 * threads, s>>>(a);
+    return cudaGetLastError();
+  }
   const size_t smem = sizeof(float4) * 2 * threads;
   particle_step_kernel<<<ngroups, threads, smem, s>>>(a);
   return cudaGetLastError();
@@ -1462,6 +1698,16 @@ cudaError_t launch_spread_field(const Geom& g, const TileLists& t, int last_step
                                 cudaStream_t s) {
   dim3 grid(g.ntx, g.nty, g.ntz);
   spread_field_kernel<<<grid, FLUID_THREADS, 0, s>>>(g, t, last_step, out, err);
+  return cudaGetLastError();
+}
+
+__global__ void widen_kernel(const float* __restrict__ in, double* __restrict__ out, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    out[k] = in[k];
+}
+
+cudaError_t launch_widen(const float* in, double* out, long long n, cudaStream_t s) {
+  widen_kernel<<<1184, 256, 0, s>>>(in, out, n);
   return cudaGetLastError();
 }
 

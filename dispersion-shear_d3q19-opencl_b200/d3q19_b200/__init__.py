@@ -70,7 +70,7 @@ class HostParams(C.Structure):
                 ("UseConstantViscosity", C.c_int), ("PointsOverride", C.c_int), ("FixedParticles", C.c_int),
                 ("ParticleSeed", C.c_uint), ("MinParticleGap", C.c_float), ("TauMax", C.c_float),
                 ("TauMin", C.c_float), ("CassonReg", C.c_float), ("Collision", C.c_int), ("Storage", C.c_int),
-                ("ParticlePrecision", C.c_int), ("Arithmetic", C.c_int)]
+                ("ParticlePrecision", C.c_int), ("Arithmetic", C.c_int), ("Fp64Build", C.c_int)]
 
 
 class Config(C.Structure):
@@ -118,6 +118,7 @@ def cuda_lib():
                                            C.POINTER(C.c_int)]
         lib.d3q19_run.argtypes = [P, C.c_int, C.c_int]
         lib.d3q19_write_periodic_map.argtypes = [P, P, C.c_int]
+        lib.d3q19_read_parkin64.restype = C.c_int
         lib.d3q19_context_bytes.argtypes = [C.POINTER(IntParams), C.POINTER(Options), C.POINTER(C.c_size_t)]
         lib.d3q19_pool_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]
         lib.d3q19_pool_admit.argtypes = [P, C.POINTER(IntParams), C.POINTER(FlpParams), C.POINTER(Options)] + \
@@ -338,6 +339,10 @@ class Simulation:
 
     def read_parkin(self):
         return self._read("d3q19_read_parkin", 16 * self.np)
+
+    def read_parkin64(self):
+        """The FP64 sphere state (particle_precision = 1 or the FP64 build)."""
+        return self._read("d3q19_read_parkin64", 16 * self.np, np.float64)
 
     def read_parforce(self):
         return self._read("d3q19_read_parforce", 8 * self.np)

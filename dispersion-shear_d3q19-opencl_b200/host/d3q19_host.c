@@ -81,6 +81,7 @@ static const keyword_t KEYWORDS[] = {
     {"storage_precision", T_INT, HPO(Storage), "0"},
     {"particle_precision", T_INT, HPO(ParticlePrecision), "0"},
     {"reference_arithmetic", T_INT, HPO(Arithmetic), "0"},
+    {"fp64_build", T_INT, HPO(Fp64Build), "0"},
 };
 #define NKEYWORDS ((int)(sizeof(KEYWORDS) / sizeof(KEYWORDS[0])))
 
@@ -320,6 +321,12 @@ void d3q19h_work_groups(d3q19h_config* cfg, int wg) {
   int workSize = 1;
   for (int i = 0; i < power2; i++) workSize *= 2;
   cfg->ip.PointsPerWorkGroup = workSize > cfg->ip.PointsPerParticle ? cfg->ip.PointsPerParticle : workSize;
+  /* New: a marker count the work-group size does not divide (384, 320, 448
+   * of the shipped partitions with a 256 work group) gets the largest power
+   * of two below it that does, where the reference's NDRange would be
+   * invalid; every count the reference runs keeps its work-group size. */
+  while (cfg->ip.PointsPerWorkGroup > 1 && cfg->ip.PointsPerParticle % cfg->ip.PointsPerWorkGroup != 0)
+    cfg->ip.PointsPerWorkGroup /= 2;
   cfg->ip.WorkGroupsPerParticle = cfg->ip.PointsPerWorkGroup > 0
                                       ? cfg->ip.PointsPerParticle / cfg->ip.PointsPerWorkGroup
                                       : 0;
@@ -708,6 +715,6 @@ void d3q19h_options(const d3q19h_config* cfg, d3q19_options* o) {
   for (int d = 0; d < 3; d++) o->tangential_vel_bc[d] = cfg->hp.TangentialVelBC[d];
   o->tau_max = cfg->hp.TauMax;
   o->tau_min = cfg->hp.TauMin;
-  o->arithmetic = cfg->hp.Arithmetic;
+  o->arithmetic = cfg->hp.Fp64Build ? 2 : cfg->hp.Arithmetic;
   o->casson_reg = cfg->hp.CassonReg;
 }

@@ -93,7 +93,9 @@ typedef struct {
    * f_i - w_i with FP32 arithmetic. */
   int storage;
   /* 0: FP32 particle state and sums in the reference's order.
-   * 1: FP64 per-sphere force/torque sums and Newton-Euler integration. */
+   * 1: FP64 sphere state, marker positions, interpolation and forces, the
+   * per-sphere force/torque sums and the Newton-Euler integration (the
+   * float read-backs hold rounded copies; d3q19_read_parkin64 the state). */
   int particle_precision;
   /* 1: spheres keep their initial position and velocity (forces are still
    * computed and reported). */
@@ -124,7 +126,10 @@ typedef struct {
    * floating-point evaluation order (both transforms as written, no
    * contraction, slot-ordered spreading, contact forces summed in the
    * reference's order): the reference's results bit for bit from the same
-   * state, except where a pow() of the viscosity law rounds differently. */
+   * state, except where a pow() of the viscosity law rounds differently.
+   * 2: the FP64 build of the fast kernels (FP64 distributions, arithmetic,
+   * local tau, spread smoothing, and particle_precision 1): the oracle the
+   * FP32 and 16-bit forms are measured against; the reference's MRT only. */
   int arithmetic;
 } d3q19_options;
 
@@ -198,6 +203,9 @@ int d3q19_read_u(d3q19_ctx* ctx, float* u);
 int d3q19_read_tau(d3q19_ctx* ctx, float* tau_lb);
 int d3q19_read_parkin(d3q19_ctx* ctx, float* parKin);
 int d3q19_read_parforce(d3q19_ctx* ctx, float* parForce);
+/* The FP64 sphere state (particle_precision = 1): double[16*np] in the
+ * parKin layout.  No counterpart in the reference (its state is float). */
+int d3q19_read_parkin64(d3q19_ctx* ctx, double* parKin);
 int d3q19_read_parfluidforce(d3q19_ctx* ctx, float* parFluidForce);
 /* The distribution buffer the last step wrote, as the reference holds it
  * after the boundary kernels (interior nodes; buffer-layer nodes are 0). */
