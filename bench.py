@@ -200,6 +200,23 @@ def setup(workload, device, storage="fp32"):
     return d3, hs, sim
 
 
+def max_over_ranks(x, dist, device):
+    """The largest x over all ranks (the job's time is its slowest rank's)."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_mlups(world, interior, steps, ms_max):
+    """Whole-job throughput of `world` independent replicas, each advancing
+    `interior` nodes by `steps` steps, timed by the slowest rank."""
+    return world * interior * steps / (ms_max * 1e-3) / 1e6
+
+
 def launches(ip, rebuild, t0, k):
     """Kernels one step sequence launches: the fluid step, and with spheres
     the particle pass, the contact forces and (every rebuild steps) the zone
@@ -247,10 +264,7 @@ def run_ours(args, rank, world, local_rank, dist):
     ms = e0.elapsed_time(e1)
     t += args.steps
     n_launch = launches(ip, R, t - args.steps, args.steps)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, dist, f"cuda:{local_rank}")
 
     # Per-launch device time of the collide-stream kernel (events around
     # each launch on the library's stream), for the roofline.
@@ -292,10 +306,7 @@ def run_ours(args, rank, world, local_rank, dist):
         rk[:] = sim2.read_parkin()
         rpff[:] = sim2.read_parfluidforce()
     e2e_s = time.perf_counter() - w0
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
-    if dist:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_s = float(e2e_t.item())
+    e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local_rank}")
     h2d = hf.nbytes + hu.nbytes + htau.nbytes + hk.nbytes + hpf.nbytes + hpff.nbytes + hsp.nbytes
     d2h = ru.nbytes + (rk.nbytes + rpff.nbytes if sim2.np > 0 else 0)
     sim2.close()
@@ -305,7 +316,7 @@ def run_ours(args, rank, world, local_rank, dist):
         return None
     peak, peak_kind = measured_peak()
     achieved = bytes_per_node * interior / (fluid_avg * 1e-3) / 1e9
-    value = world * interior * args.steps / (ms_max * 1e-3) / 1e6
+    value = replica_mlups(world, interior, args.steps, ms_max)
     out = {
         "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5), "higher_is_better": True,
@@ -323,7 +334,7 @@ def run_ours(args, rank, world, local_rank, dist):
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                      "fallback 6.65 TB/s",
                      "step_frac": round(value / world * 1e6 * bytes_per_node / 1e9 / peak, 4)},
-        "e2e": {"value": round(world * interior * args.steps / e2e_s / 1e6, 1), "unit": "MLUPS",
+        "e2e": {"value": round(replica_mlups(world, interior, args.steps, e2e_s * 1e3), 1), "unit": "MLUPS",
                 "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                 "note": "C-ABI calls from pinned host buffers: upload of the initial state, K steps, read-back "
                         "of u, sphere kinematics and forces"},
