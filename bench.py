@@ -530,7 +530,7 @@ def run_served(args):
     alone = sv.summary(base, bwall)
     by = {r.rid: r for r in base}
     visc_err = [abs(r.eff_viscosity - by[r.rid].eff_viscosity) / max(abs(by[r.rid].eff_viscosity), 1e-30)
-                for r in recs]
+                for r in recs if not (r.failed or by[r.rid].failed)]
     return {"metric": "solves/s (served sweep)", "value": round(served["solves_per_s"], 3), "unit": "solves/s",
             "n_gpus": 1, "higher_is_better": True, "dtype": "f32 arithmetic, f16 shifted storage",
             "data": "synthetic (seeded Poisson arrivals)", "impl": "ours",

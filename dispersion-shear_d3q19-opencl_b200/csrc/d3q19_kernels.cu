@@ -564,6 +564,8 @@ __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& t
   // value = (hi * 2^16 + lo) * 2^-k, both parts scaled exactly by powers of
   // two and joined with one rounding (exactly in FP64).  All sums are read
   // before the field overwrites them.
+  const float inv = ldexpf(1.0f, -k), inv_hi = ldexpf(1.0f, 16 - k);
+  const double inv64 = ldexp(1.0, -k), inv_hi64 = ldexp(1.0, 16 - k);
   R v[SPREAD_CONVERT_PER_THREAD];
 #pragma unroll
   for (int r = 0; r < SPREAD_CONVERT_PER_THREAD; r++) {
@@ -572,9 +574,9 @@ __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& t
     if (h < 3 * HALO_N) {
       const unsigned* slot = reinterpret_cast<const unsigned*>(&(&s.acc[0][0])[h]);
       if (sizeof(R) == 4)
-        v[r] = __fmaf_rn((float)(int)slot[1], ldexpf(1.0f, 16 - k), (float)slot[0] * ldexpf(1.0f, -k));
+        v[r] = __fmaf_rn((float)(int)slot[1], inv_hi, (float)slot[0] * inv);
       else
-        v[r] = (R)(ldexp((double)(int)slot[1], 16 - k) + ldexp((double)slot[0], -k));
+        v[r] = (R)((double)(int)slot[1] * inv_hi64 + (double)slot[0] * inv64);
     }
   }
   __syncthreads();

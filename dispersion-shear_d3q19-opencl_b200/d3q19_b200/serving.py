@@ -23,7 +23,7 @@ import time
 
 import numpy as np
 
-from . import HostState, Options, Pool, Simulation, keywords_text, parse_config
+from . import D3Q19Error, HostState, Options, Pool, Simulation, keywords_text, parse_config
 
 MODELS = ("newtonian", "power_law", "casson")
 
@@ -111,6 +111,7 @@ class SolveRecord:
     stress: float
     eff_viscosity: float
     converged: bool
+    failed: bool = False  # the solve stopped on a device error (non-finite state)
 
     @property
     def latency(self) -> float:
@@ -138,6 +139,7 @@ def summary(records: list, wall: float) -> dict:
             "p50_latency_s": float(np.percentile(lat, 50)) if len(lat) else None,
             "p99_latency_s": float(np.percentile(lat, 99)) if len(lat) else None,
             "converged": int(sum(r.converged for r in records)),
+            "failed": int(sum(r.failed for r in records)),
             "steps": int(sum(r.steps for r in records))}
 
 
@@ -195,8 +197,17 @@ class Server:
             for slot in list(active):
                 req, start, conv = active[slot]
                 m = self.pool.member(slot)
-                stress, _, visc = m.mean_stress()
                 steps = self.pool.steps(slot)
+                try:
+                    stress, _, visc = m.mean_stress()
+                except D3Q19Error:
+                    # A member whose state went non-finite retires as failed;
+                    # the others are independent of it.
+                    done.append(SolveRecord(req.rid, req.arrival, start, self.clock() - t0, steps, float("nan"),
+                                            float("nan"), False, True))
+                    self.pool.release(slot)
+                    del active[slot]
+                    continue
                 ok = conv.update(stress)
                 if ok or steps >= self.max_steps:
                     done.append(SolveRecord(req.rid, req.arrival, start, self.clock() - t0, steps, stress, visc, ok))
@@ -221,17 +232,22 @@ def one_at_a_time(requests: list, storage: int = 0, check_every: int = 500, rel_
         hs = build(req)
         sim = Simulation.from_host_state(hs, device=device, storage=storage)
         conv = Convergence(rel_tol)
-        t, ok = 1, False
+        t, ok, failed = 1, False, False
         stress = visc = 0.0
         while t - 1 < max_steps:
             sim.run(t, check_every)
             t += check_every
-            stress, _, visc = sim.mean_stress()
+            try:
+                stress, _, visc = sim.mean_stress()
+            except D3Q19Error:
+                stress = visc = float("nan")
+                failed = True
+                break
             if conv.update(stress):
                 ok = True
                 break
         sim.close()
-        done.append(SolveRecord(req.rid, req.arrival, start, clock() - t0, t - 1, stress, visc, ok))
+        done.append(SolveRecord(req.rid, req.arrival, start, clock() - t0, t - 1, stress, visc, ok, failed))
     return done, clock() - t0
 
 

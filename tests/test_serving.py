@@ -123,3 +123,23 @@ def test_context_bytes_counts_the_distributions():
     b16 = d3.context_bytes(cfg.ip, o)
     nc = 64 ** 3
     assert b32 >= 2 * 19 * 4 * nc + 16 * nc and b32 - b16 == pytest.approx(2 * 19 * 2 * nc, rel=1e-3)
+
+
+class FailingMember(FakeMember):
+    def mean_stress(self):
+        if self.pool.steps_done[self.slot] > 1000:
+            raise d3.D3Q19Error("mean_stress: ENUMERIC: non-finite")
+        return super().mean_stress()
+
+
+def test_server_retires_a_failed_member_and_goes_on():
+    reqs = [sv.ShearRequest(rid=i, edge=(32, 32, 32), phi=0.0, model="newtonian", wall_speed=0.02, seed=1,
+                            arrival=0.0) for i in range(3)]
+    pool = FakePool(budget=100)
+    orig = pool.member
+    pool.member = lambda s: FailingMember(pool, s, pool.target[s]) if s == 1 else orig(s)
+    recs, wall = sv.Server(pool, check_every=500, max_steps=30000, clock=lambda: 0.0, sleep=lambda dt: None).run(
+        reqs, build=lambda r: {"bytes": 10, "rid": r.rid, "target": 1.0})
+    by = {r.rid: r for r in recs}
+    assert by[1].failed and not by[1].converged and by[0].converged and by[2].converged
+    assert sv.summary(recs, 1.0)["failed"] == 1 and pool.used == 0
