@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -1105,6 +1106,8 @@ struct d3q19_pool {
   int part_threads = 128;
   bool dirty = true;
   int fblocks = 0, pblocks = 0, cblocks = 0;
+  double* d_stats = nullptr;  // per-member plane sums and error words (d3q19_pool_mean_stress)
+  size_t stats_cap = 0;
   std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  // (steps, fblocks, pblocks, cblocks)
   long long steps = 0;
   char msg[512] = {0};
@@ -1357,6 +1360,68 @@ extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
   return 0;
 }
 
+extern "C" int d3q19_pool_mean_stress(d3q19_pool* p, double* stress_xz, double* shear_rate, double* eff_viscosity,
+                                      int* status) {
+  if (!p || !stress_xz || !status) return D3Q19_EINVAL;
+  cudaSetDevice(p->dev);
+  // Layout: per member, 5*Nz plane sums then its error word.
+  std::vector<size_t> off(p->max_slots, 0);
+  size_t need = 0;
+  for (int s = 0; s < p->max_slots; s++)
+    if (p->slot[s]) {
+      off[s] = need;
+      need += 5 * (size_t)p->slot[s]->g.Nz + 1;
+    }
+  if (need > p->stats_cap) {
+    POOL_TRY(p, cudaStreamSynchronize(p->stream));
+    if (p->d_stats) cudaFree(p->d_stats);
+    p->d_stats = nullptr;
+    p->stats_cap = 0;
+    POOL_TRY(p, cudaMalloc(&p->d_stats, sizeof(double) * (need + 1024)));
+    p->stats_cap = need + 1024;
+  }
+  for (int s = 0; s < p->max_slots; s++) {
+    d3q19_ctx* c = p->slot[s];
+    if (!c) continue;
+    if (int rc = join_side(c)) return pfail(p, rc, "%s", d3q19_last_error(c));
+    POOL_TRY(p, cudaEventRecord(c->ev_fork, c->stream));
+    POOL_TRY(p, cudaStreamWaitEvent(p->stream, c->ev_fork, 0));
+    POOL_TRY(p, launch_plane_stats(c->g, c->u, c->tau, c->fp.NewtonianTau, c->opt.variable_viscosity,
+                                   p->d_stats + off[s], p->stream));
+    POOL_TRY(p, launch_copy_err(c->err, p->d_stats + off[s] + 5 * (size_t)c->g.Nz, p->stream));
+  }
+  std::vector<double> h(std::max<size_t>(need, 1));
+  POOL_TRY(p, cudaStreamSynchronize(p->stream));
+  if (need) POOL_TRY(p, cudaMemcpy(h.data(), p->d_stats, sizeof(double) * need, cudaMemcpyDeviceToHost));
+  for (int s = 0; s < p->max_slots; s++) {
+    d3q19_ctx* c = p->slot[s];
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    if (!c) {
+      stress_xz[s] = nan;
+      if (shear_rate) shear_rate[s] = nan;
+      if (eff_viscosity) eff_viscosity[s] = nan;
+      status[s] = D3Q19_EINVAL;
+      continue;
+    }
+    const int Nz = c->g.Nz;
+    const unsigned e = (unsigned)h[off[s] + 5 * (size_t)Nz];
+    c->sticky |= e;
+    status[s] = (c->sticky & ERR_TILE_OVERFLOW) ? D3Q19_EOVERFLOW
+                : (c->sticky & (ERR_NONFINITE | ERR_FIXED_RANGE | ERR_ZONE_RANGE)) ? D3Q19_ENUMERIC
+                                                                                     : 0;
+    double gs = 0.0, ts = 0.0;
+    for (int z = 1; z <= Nz - 2; z++) {
+      gs += h[off[s] + 5 * (size_t)z + 3];
+      ts += h[off[s] + 5 * (size_t)z + 4];
+    }
+    const double n = (double)(c->g.Nx - 2) * (c->g.Ny - 2) * (Nz - 2);
+    stress_xz[s] = ts / n;
+    if (shear_rate) shear_rate[s] = gs / n;
+    if (eff_viscosity) eff_viscosity[s] = gs != 0.0 ? ts / gs : 0.0;
+  }
+  return 0;
+}
+
 extern "C" d3q19_ctx* d3q19_pool_context(d3q19_pool* p, int slot) {
   if (!p || slot < 0 || slot >= p->max_slots) return nullptr;
   return p->slot[slot];
@@ -1431,7 +1496,7 @@ extern "C" int d3q19_pool_destroy(d3q19_pool* p) {
       d3q19_destroy(c);
       c = nullptr;
     }
-  void* ptrs[] = {p->d_fargs, p->d_pargs, p->d_zargs, p->d_work, p->d_zslots, p->d_counts};
+  void* ptrs[] = {p->d_fargs, p->d_pargs, p->d_zargs, p->d_work, p->d_zslots, p->d_counts, p->d_stats};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->ev_done) cudaEventDestroy(p->ev_done);

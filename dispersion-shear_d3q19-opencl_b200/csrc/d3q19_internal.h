@@ -180,6 +180,8 @@ cudaError_t launch_marker_cells(const float4* mrec, int M, int* cells, cudaStrea
 // shear stress: out[5 * Nz].
 cudaError_t launch_plane_stats(const Geom& g, const float* u, const float* tau, float tauN, int variable,
                                double* out, cudaStream_t s);
+// *out = the device error word (as a double), for batched status reads.
+cudaError_t launch_copy_err(const unsigned* err, double* out, cudaStream_t s);
 // Reference-exact variants (d3q19_exact.cu, compiled without contraction).
 cudaError_t launch_fluid_exact(const FluidArgs& a, bool first, bool variable, int slots, cudaStream_t s);
 cudaError_t launch_spread_field_exact(const Geom& g, const TileLists& t, int slots, float* out, unsigned* err,

@@ -1713,6 +1713,13 @@ cudaError_t launch_widen(const float* in, double* out, long long n, cudaStream_t
   return cudaGetLastError();
 }
 
+__global__ void copy_err_kernel(const unsigned* err, double* out) { *out = (double)*err; }
+
+cudaError_t launch_copy_err(const unsigned* err, double* out, cudaStream_t s) {
+  copy_err_kernel<<<1, 1, 0, s>>>(err, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_plane_stats(const Geom& g, const float* u, const float* tau, float tauN, int variable,
                                double* out, cudaStream_t s) {
   plane_stats_kernel<<<g.Nz, 256, 0, s>>>(g, u, tau, tauN, variable, out);

@@ -138,6 +138,7 @@ def cuda_lib():
         lib.d3q19_pool_last_error.restype = C.c_char_p
         lib.d3q19_pool_last_error.argtypes = [P]
         lib.d3q19_pool_destroy.argtypes = [P]
+        lib.d3q19_pool_mean_stress.argtypes = [P, P, P, P, P]
         _cuda = lib
     return _cuda
 
@@ -447,6 +448,7 @@ class Pool:
             raise D3Q19Error(f"d3q19_pool_create: {STATUS.get(rc, rc)}: {self.lib.d3q19_pool_last_error(None).decode()}")
         self.h = h
         self.storage = storage
+        self.max_slots = max_slots
         self.rebuild_freq = rebuild_freq
         self.period = 2 // math.gcd(2, rebuild_freq) * rebuild_freq
         self.members = {}
@@ -491,6 +493,16 @@ class Pool:
             raise D3Q19Error(f"pool slot {slot} is free")
         ip, fp, opt = self.members[slot]
         return Simulation._view(self.lib, C.c_void_p(hnd), ip, fp, opt)
+
+    def mean_stress_all(self, max_slots: int):
+        """(stress, shear rate, effective viscosity, status) of every slot in one
+        pass; status 0 for a healthy member, a negative code for a member
+        whose state went non-finite, EINVAL (-1) for a free slot."""
+        st, ra, vi = (np.zeros(max_slots, np.float64) for _ in range(3))
+        code = np.zeros(max_slots, np.int32)
+        self._check(self.lib.d3q19_pool_mean_stress(self.h, _ptr(st), _ptr(ra), _ptr(vi), _ptr(code)),
+                    "pool_mean_stress")
+        return st, ra, vi, code
 
     def steps(self, slot: int) -> int:
         return int(self.lib.d3q19_pool_slot_steps(self.h, slot))

@@ -20,6 +20,7 @@ from __future__ import annotations
 import dataclasses
 import math
 import time
+from concurrent.futures import Future, ThreadPoolExecutor
 
 import numpy as np
 
@@ -146,10 +147,12 @@ def summary(records: list, wall: float) -> dict:
 class Server:
     """Continuous batching over a Pool: admit on arrival while slots and
     budget last, advance every member `check_every` steps at a time, retire
-    the converged ones."""
+    the converged ones.  The host-side set-up of an arrived request (input
+    parsing, sphere placement, initial state) runs on `builders` worker
+    threads while the GPU works."""
 
     def __init__(self, pool: Pool, check_every: int = 500, rel_tol: float = 1e-4, max_steps: int = 20000,
-                 clock=time.perf_counter, sleep=time.sleep):
+                 clock=time.perf_counter, sleep=time.sleep, builders: int = 4):
         if check_every % pool.period:
             raise ValueError(f"check_every must be a multiple of the pool period {pool.period}")
         self.pool = pool
@@ -158,6 +161,23 @@ class Server:
         self.max_steps = max_steps
         self.clock = clock
         self.sleep = sleep
+        self.builders = builders
+
+    def _stresses(self, active):
+        """{slot: (stress, viscosity) or None for a failed member}."""
+        out = {}
+        if hasattr(self.pool, "mean_stress_all"):
+            st, _, vi, code = self.pool.mean_stress_all(self.pool.max_slots)
+            for slot in active:
+                out[slot] = None if code[slot] != 0 else (float(st[slot]), float(vi[slot]))
+            return out
+        for slot in active:
+            try:
+                stress, _, visc = self.pool.member(slot).mean_stress()
+                out[slot] = (stress, visc)
+            except D3Q19Error:
+                out[slot] = None
+        return out
 
     def run(self, requests: list, build=host_state) -> tuple:
         """Serves the requests (arrival times relative to the call); returns
@@ -167,53 +187,81 @@ class Server:
         active = {}  # slot -> (request, start time, Convergence)
         joining = {}  # admitted while the pool was running: join the next chunk
         done = []
-        qi = 0
+        ex = ThreadPoolExecutor(max_workers=self.builders) if self.builders > 0 else None
+        built = {}  # rid -> Future or host state of an arrived request
+        qi = nb = 0
+
+        def prepare():
+            # Start the set-up of every request that has arrived.
+            nonlocal nb
+            now = self.clock() - t0
+            while nb < len(queue) and queue[nb].arrival <= now:
+                req = queue[nb]
+                built[req.rid] = ex.submit(build, req) if ex else build(req)
+                nb += 1
 
         def admit_arrived():
             # Admit in arrival order; stop at the first one that does not fit.
             nonlocal qi
-            while qi < len(queue) and queue[qi].arrival <= self.clock() - t0:
+            prepare()
+            while qi < nb:
                 req = queue[qi]
-                slot = self.pool.admit(build(req))
+                hs = built[req.rid]
+                if ex:
+                    hs = hs.result()
+                slot = self.pool.admit(hs)
                 if slot is None:
+                    built[req.rid] = hs if not ex else _done_future(hs)
                     if not active and not joining:
                         raise RuntimeError(f"request {req.rid} does not fit an empty pool")
                     return
+                del built[req.rid]
                 joining[slot] = (req, self.clock() - t0, Convergence(self.rel_tol))
                 qi += 1
 
-        while qi < len(queue) or active or joining:
-            admit_arrived()
-            active.update(joining)
-            joining.clear()
-            if not active:
-                self.sleep(max(0.0, queue[qi].arrival - (self.clock() - t0)))
-                continue
-            # The chunk runs on the pool's stream while the host admits the
-            # requests that arrived meanwhile (their set-up and first steps
-            # overlap the chunk on the device); they join the next chunk.
-            self.pool.advance(self.check_every)
-            admit_arrived()
-            for slot in list(active):
-                req, start, conv = active[slot]
-                m = self.pool.member(slot)
-                steps = self.pool.steps(slot)
-                try:
-                    stress, _, visc = m.mean_stress()
-                except D3Q19Error:
-                    # A member whose state went non-finite retires as failed;
-                    # the others are independent of it.
-                    done.append(SolveRecord(req.rid, req.arrival, start, self.clock() - t0, steps, float("nan"),
-                                            float("nan"), False, True))
-                    self.pool.release(slot)
-                    del active[slot]
+        try:
+            while qi < len(queue) or active or joining:
+                admit_arrived()
+                active.update(joining)
+                joining.clear()
+                if not active:
+                    self.sleep(max(0.0, queue[qi].arrival - (self.clock() - t0)))
                     continue
-                ok = conv.update(stress)
-                if ok or steps >= self.max_steps:
-                    done.append(SolveRecord(req.rid, req.arrival, start, self.clock() - t0, steps, stress, visc, ok))
-                    self.pool.release(slot)
-                    del active[slot]
+                # The chunk runs on the pool's stream while the host admits the
+                # requests that arrived meanwhile (their set-up and first steps
+                # overlap the chunk on the device); they join the next chunk.
+                self.pool.advance(self.check_every)
+                admit_arrived()
+                stresses = self._stresses(active)
+                for slot in list(active):
+                    req, start, conv = active[slot]
+                    steps = self.pool.steps(slot)
+                    res = stresses[slot]
+                    if res is None:
+                        # A member whose state went non-finite retires as failed;
+                        # the others are independent of it.
+                        done.append(SolveRecord(req.rid, req.arrival, start, self.clock() - t0, steps, float("nan"),
+                                                float("nan"), False, True))
+                        self.pool.release(slot)
+                        del active[slot]
+                        continue
+                    stress, visc = res
+                    ok = conv.update(stress)
+                    if ok or steps >= self.max_steps:
+                        done.append(SolveRecord(req.rid, req.arrival, start, self.clock() - t0, steps, stress, visc,
+                                                ok))
+                        self.pool.release(slot)
+                        del active[slot]
+        finally:
+            if ex:
+                ex.shutdown(wait=True)
         return done, self.clock() - t0
+
+
+def _done_future(value):
+    f = Future()
+    f.set_result(value)
+    return f
 
 
 def one_at_a_time(requests: list, storage: int = 0, check_every: int = 500, rel_tol: float = 1e-4,

@@ -317,6 +317,12 @@ int d3q19_pool_advance(d3q19_pool* pool, int nsteps);
 d3q19_ctx* d3q19_pool_context(d3q19_pool* pool, int slot);
 /* Steps the member has taken, or -1 for a free slot. */
 long long d3q19_pool_slot_steps(d3q19_pool* pool, int slot);
+/* d3q19_mean_stress of every member in one pass on the pool's stream (one
+ * read-back for all): arrays of max_slots entries; status[s] is 0, the
+ * member's D3Q19_ENUMERIC / D3Q19_EOVERFLOW device error, or D3Q19_EINVAL
+ * for a free slot (values NaN). */
+int d3q19_pool_mean_stress(d3q19_pool* pool, double* stress_xz, double* shear_rate, double* eff_viscosity,
+                           int* status);
 /* Frees the member's slot and device memory. */
 int d3q19_pool_release(d3q19_pool* pool, int slot);
 /* Budget in use, the budget, and the member count. */

@@ -125,3 +125,17 @@ def test_server_serves_a_burst():
     assert pool.usage()[2] == 0
     assert all(r.steps <= 600 + pool.period and np.isfinite(r.stress) for r in recs)
     pool.close()
+
+
+def test_batched_stress_matches_per_member():
+    pool = d3.Pool(storage=1, max_slots=6)
+    slots = [pool.admit(sv.host_state(r)) for r in REQS]
+    pool.advance(100)
+    st, ra, vi, code = pool.mean_stress_all(6)
+    for s in slots:
+        one = pool.member(s).mean_stress()
+        assert code[s] == 0
+        assert (st[s], ra[s], vi[s]) == one
+    free = [k for k in range(6) if k not in slots]
+    assert all(code[k] == -1 and np.isnan(st[k]) for k in free)
+    pool.close()
