@@ -34,6 +34,10 @@ struct d3q19_ctx {
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool side_pending = false;
+  // Pass-by-pass stepping (d3q19_k_*): 0 next is the collide-stream pass,
+  // 1 the particle pass, 2 the contacts of step kt.
+  int kstage = 0;
+  int kt = 0;
   Geom g;
   FluidParams fpar;
   ParticleParams ppar;
@@ -631,6 +635,61 @@ static int enqueue_step(d3q19_ctx* c, int t) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// The step pass by pass, in the reference's kernel order (sim_main.c:324-447),
+// all on the context's stream.
+extern "C" int d3q19_k_collide_stream(d3q19_ctx* c, int t) {
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if (c->kstage != 0) return fail(c, D3Q19_ESTATE, "the particle pass of step %d comes first", c->kt);
+  cudaSetDevice(c->dev);
+  if (c->side_pending) CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+  c->side_pending = false;
+  const FluidArgs fa = fluid_args(c, t, c->cur);
+  if (c->opt.arithmetic == 1)
+    CUDA_TRY(c, launch_fluid_exact(fa, c->f_state == 1, c->opt.variable_viscosity != 0, c->ip.MaxSurfPointsPerNode,
+                                   c->stream));
+  else
+    CUDA_TRY(c, launch_fluid(fa, c->f_state == 1, c->opt.variable_viscosity != 0, c->opt.collision, c->opt.storage,
+                             c->stream));
+  c->cur = 1 - c->cur;
+  c->f_state = 2;
+  c->last_t = t;
+  c->kt = t;
+  c->kstage = c->ppar.np > 0 ? 1 : 0;
+  return 0;
+}
+
+extern "C" int d3q19_k_particles(d3q19_ctx* c, int t) {
+  if (!c) return D3Q19_EINVAL;
+  if (c->ppar.np == 0) return 0;
+  if (c->kstage != 1 || t != c->kt) return fail(c, D3Q19_ESTATE, "the collide-stream pass of step %d comes first", t);
+  cudaSetDevice(c->dev);
+  CUDA_TRY(c, launch_particles(particle_args(c, t, c->pcur), c->stream));
+  c->kstage = 2;
+  return 0;
+}
+
+extern "C" int d3q19_k_contacts(d3q19_ctx* c, int t) {
+  if (!c) return D3Q19_EINVAL;
+  if (c->ppar.np == 0) return 0;
+  if (c->kstage != 2 || t != c->kt) return fail(c, D3Q19_ESTATE, "the particle pass of step %d comes first", t);
+  cudaSetDevice(c->dev);
+  CUDA_TRY(c, launch_contacts(particle_args(c, t, c->pcur), c->stream));
+  c->pcur = 1 - c->pcur;
+  c->kstage = 0;
+  return 0;
+}
+
+extern "C" int d3q19_k_zones(d3q19_ctx* c) {
+  if (!c) return D3Q19_EINVAL;
+  if (c->ppar.np == 0) return 0;
+  if (c->kstage != 0) return fail(c, D3Q19_ESTATE, "the contacts of step %d come first", c->kt);
+  cudaSetDevice(c->dev);
+  CUDA_TRY(c, launch_zones(zone_args(c, c->pcur), c->stream));
+  return 0;
+}
+
 // Orders the side stream's pending work (contacts, zone rebuild) before
 // whatever the main stream runs next.
 static int join_side(d3q19_ctx* c) {
@@ -643,6 +702,7 @@ static int join_side(d3q19_ctx* c) {
 extern "C" int d3q19_step(d3q19_ctx* c, int t) {
   int rc = check_ready(c);
   if (rc) return rc;
+  if (c->kstage != 0) return fail(c, D3Q19_ESTATE, "step %d was left between passes", c->kt);
   cudaSetDevice(c->dev);
   if ((rc = enqueue_step(c, t))) return rc;
   return join_side(c);
@@ -653,6 +713,7 @@ static int gcd_i(int a, int b) { return b ? gcd_i(b, a % b) : a; }
 extern "C" int d3q19_run(d3q19_ctx* c, int t0, int nsteps) {
   int rc = check_ready(c);
   if (rc) return rc;
+  if (c->kstage != 0) return fail(c, D3Q19_ESTATE, "step %d was left between passes", c->kt);
   cudaSetDevice(c->dev);
   // The launch sequence repeats with period Lp in t (buffer parity and the
   // zone-rebuild schedule), so a captured chunk of CH steps replays at any

@@ -117,6 +117,9 @@ def cuda_lib():
         lib.d3q19_profile_read.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_double),
                                            C.POINTER(C.c_int)]
         lib.d3q19_run.argtypes = [P, C.c_int, C.c_int]
+        for name in ("d3q19_k_collide_stream", "d3q19_k_particles", "d3q19_k_contacts"):
+            getattr(lib, name).argtypes = [P, C.c_int]
+        lib.d3q19_k_zones.argtypes = [P]
         lib.d3q19_write_periodic_map.argtypes = [P, P, C.c_int]
         lib.d3q19_read_parkin64.restype = C.c_int
         lib.d3q19_context_bytes.argtypes = [C.POINTER(IntParams), C.POINTER(Options), C.POINTER(C.c_size_t)]
@@ -317,6 +320,14 @@ class Simulation:
 
     def step(self, t: int):
         self._check(self.lib.d3q19_step(self.h, t), "step")
+
+    def step_by_pass(self, t: int, rebuild: bool):
+        """Step t through the pass entry points (d3q19_k_*), in order."""
+        self._check(self.lib.d3q19_k_collide_stream(self.h, t), "k_collide_stream")
+        self._check(self.lib.d3q19_k_particles(self.h, t), "k_particles")
+        self._check(self.lib.d3q19_k_contacts(self.h, t), "k_contacts")
+        if rebuild:
+            self._check(self.lib.d3q19_k_zones(self.h), "k_zones")
 
     def run(self, t0: int, n: int):
         self._check(self.lib.d3q19_run(self.h, t0, n), "run")

@@ -191,6 +191,23 @@ int d3q19_write_periodic_map(d3q19_ctx* ctx, const int* strMap, int numPeriodicN
  * Asynchronous on the context's stream. */
 int d3q19_step(d3q19_ctx* ctx, int t);
 
+/* The step in its passes, for kernel-level use; calling them in this order
+ * for step t is d3q19_step(ctx, t) (bit for bit), all on the context's
+ * stream.  Out-of-order calls return D3Q19_ESTATE.
+ *   d3q19_k_collide_stream: collideMRT_stream_D3Q19 + boundary_periodic +
+ *     boundary_velocity + the reset and slot sum of the spread force of step
+ *     t-1 (GPU_program.cl:258-865), fused;
+ *   d3q19_k_particles: particle_dynamics + particle_fluid_forces_linear_stencil
+ *     (CPU_program.cl:187-277, GPU_program.cl:81-256);
+ *   d3q19_k_contacts: particle_particle_forces (CPU_program.cl:76-184);
+ *   d3q19_k_zones: update_particle_zones (CPU_program.cl:280-315), after the
+ *     contacts of steps with t % rebuild_neigh_list_freq == 0.
+ * The particle passes do nothing without spheres. */
+int d3q19_k_collide_stream(d3q19_ctx* ctx, int t);
+int d3q19_k_particles(d3q19_ctx* ctx, int t);
+int d3q19_k_contacts(d3q19_ctx* ctx, int t);
+int d3q19_k_zones(d3q19_ctx* ctx);
+
 /* Steps t0 .. t0+nsteps-1, replayed from captured CUDA graphs. */
 int d3q19_run(d3q19_ctx* ctx, int t0, int nsteps);
 

@@ -163,3 +163,30 @@ def test_reference_exact_arithmetic_bitwise(name):
         return
     for k in got:
         _assert_bitwise(got[k], ref[k], k)
+
+
+def test_pass_by_pass_steps_match_step():
+    """The pass entry points (d3q19_k_*) in the reference's order give the
+    state d3q19_step gives, bit for bit; out-of-order calls are refused."""
+    import d3q19_b200 as d3
+    case = CASES["contacts"]
+    g = load_golden("contacts")
+    a, ip, _ = sim_from_golden(g, case)
+    b, _, _ = sim_from_golden(g, case)
+    R = int(case.get("rebuild_neigh_list_freq", 10))
+    for t in range(1, 25):
+        a.step(t)
+        b.step_by_pass(t, t % R == 0)
+    for rd in ("read_u", "read_parkin", "read_parfluidforce", "read_parforce", "read_spread_force"):
+        x, y = getattr(a, rd)(), getattr(b, rd)()
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), rd
+    pa, za, na = a.read_zones()
+    pb, zb, nb = b.read_zones()
+    assert np.array_equal(pa, pb) and np.array_equal(na, nb)
+    with pytest.raises(d3.D3Q19Error, match="ESTATE"):
+        b._check(b.lib.d3q19_k_contacts(b.h, 25), "k_contacts")
+    b._check(b.lib.d3q19_k_collide_stream(b.h, 25), "k_collide_stream")
+    with pytest.raises(d3.D3Q19Error, match="ESTATE"):
+        b.step(26)
+    a.close()
+    b.close()
