@@ -1107,6 +1107,137 @@ extern "C" int d3q19_read_spread_force_static(d3q19_ctx* c, float* gpf0) {
 }
 
 /* ---------------------------------------------------------------------------
+ * Checkpoints: the whole device state of a context in one host buffer.
+ * ------------------------------------------------------------------------- */
+namespace {
+struct CkptHeader {
+  char magic[8];
+  int version;
+  int storage, p64, arithmetic;
+  long long NC, ntiles;
+  int np, nfa, P, cap, nzones;
+  int f_state, last_t, sticky;
+  long long clamps;
+};
+// The device blocks of a checkpoint in order: {pointer, bytes}.
+struct CkptBlock {
+  void* ptr;
+  size_t bytes;
+};
+std::vector<CkptBlock> ckpt_blocks(d3q19_ctx* c) {
+  const long long NC = c->g.NC;
+  std::vector<CkptBlock> b;
+  b.push_back({c->f[c->cur], (size_t)storage_bytes(c->opt.storage) * 19 * NC});
+  b.push_back({c->u, sizeof(float) * 3 * NC});
+  b.push_back({c->tau, sizeof(float) * NC});
+  if (c->tau64) b.push_back({c->tau64, sizeof(double) * NC});
+  const long long np = c->ppar.np;
+  if (np > 0) {
+    const long long M = np * c->ppar.P, nfa = c->ppar.nfa;
+    b.push_back({c->kin[c->pcur], sizeof(float4) * 4 * np});
+    b.push_back({c->pf[c->pcur], sizeof(float4) * 2 * np});
+    b.push_back({c->pff[c->pcur], sizeof(float4) * 2 * np * nfa});
+    if (c->kin64[0]) {
+      b.push_back({c->kin64[c->pcur], sizeof(double) * 16 * np});
+      b.push_back({c->pff64[c->pcur], sizeof(double) * 8 * np * nfa});
+    }
+    b.push_back({c->sphere, sizeof(float4) * c->ppar.P});
+    b.push_back({c->mrec, sizeof(float4) * 2 * M});
+    b.push_back({c->tile_count, sizeof(int) * c->ntiles});
+    b.push_back({c->tile_list, sizeof(int) * c->ntiles * c->tile_cap});
+    b.push_back({c->fmax, sizeof(unsigned) * 2});
+    const long long Z = c->nzones;
+    b.push_back({c->znd, sizeof(int) * 28 * Z});
+    b.push_back({c->parsZone, sizeof(int) * np});
+    b.push_back({c->zoneMembers, sizeof(int) * Z * np});
+    b.push_back({c->numParInZone, sizeof(int) * Z});
+    b.push_back({c->revStart, sizeof(int) * (Z + 1)});
+    b.push_back({c->revList, sizeof(int) * 27 * Z});
+    b.push_back({c->zoneOf, sizeof(int) * np});
+  }
+  return b;
+}
+}  // namespace
+
+extern "C" int d3q19_checkpoint_bytes(d3q19_ctx* c, size_t* bytes) {
+  if (!c || !bytes) return D3Q19_EINVAL;
+  size_t n = sizeof(CkptHeader);
+  for (const auto& b : ckpt_blocks(c)) n += b.bytes;
+  *bytes = n;
+  return 0;
+}
+
+extern "C" int d3q19_checkpoint(d3q19_ctx* c, void* buf, size_t bytes) {
+  if (!c || !buf) return D3Q19_EINVAL;
+  if (c->f_state == 0) return fail(c, D3Q19_ESTATE, "lattice not written");
+  if (c->kstage != 0) return fail(c, D3Q19_ESTATE, "step %d was left between passes", c->kt);
+  size_t need = 0;
+  d3q19_checkpoint_bytes(c, &need);
+  if (bytes < need) return fail(c, D3Q19_EINVAL, "checkpoint needs %zu bytes", need);
+  if (int rc = d3q19_synchronize(c)) return rc;  // joins the side stream, reports device errors
+  CkptHeader h;
+  memset(&h, 0, sizeof(h));
+  memcpy(h.magic, "D3Q19CK", 8);
+  h.version = 1;
+  h.storage = c->opt.storage;
+  h.p64 = c->kin64[0] != nullptr;
+  h.arithmetic = c->opt.arithmetic;
+  h.NC = c->g.NC;
+  h.ntiles = c->ntiles;
+  h.np = c->ppar.np;
+  h.nfa = c->ppar.nfa;
+  h.P = c->ppar.P;
+  h.cap = c->tile_cap;
+  h.nzones = c->nzones;
+  h.f_state = c->f_state;
+  h.last_t = c->last_t;
+  h.sticky = (int)c->sticky;
+  unsigned long long cl = 0;
+  char* p = static_cast<char*>(buf) + sizeof(h);
+  CUDA_TRY(c, cudaMemcpyAsync(&cl, c->clamps, sizeof(cl), cudaMemcpyDeviceToHost, c->stream));
+  for (const auto& b : ckpt_blocks(c)) {
+    CUDA_TRY(c, cudaMemcpyAsync(p, b.ptr, b.bytes, cudaMemcpyDeviceToHost, c->stream));
+    p += b.bytes;
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  h.clamps = (long long)cl;
+  memcpy(buf, &h, sizeof(h));
+  return 0;
+}
+
+extern "C" int d3q19_restore(d3q19_ctx* c, const void* buf, size_t bytes) {
+  if (!c || !buf || bytes < sizeof(CkptHeader)) return D3Q19_EINVAL;
+  CkptHeader h;
+  memcpy(&h, buf, sizeof(h));
+  if (memcmp(h.magic, "D3Q19CK", 8) != 0 || h.version != 1) return fail(c, D3Q19_EINVAL, "not a checkpoint");
+  if (h.storage != c->opt.storage || h.p64 != (c->kin64[0] != nullptr) || h.arithmetic != c->opt.arithmetic ||
+      h.NC != c->g.NC || h.ntiles != c->ntiles || h.np != c->ppar.np || h.nfa != c->ppar.nfa || h.P != c->ppar.P ||
+      h.cap != c->tile_cap || h.nzones != c->nzones)
+    return fail(c, D3Q19_EINVAL, "checkpoint of a context with other parameters");
+  size_t need = 0;
+  d3q19_checkpoint_bytes(c, &need);
+  if (bytes < need) return fail(c, D3Q19_EINVAL, "checkpoint truncated (%zu of %zu bytes)", bytes, need);
+  cudaSetDevice(c->dev);
+  if (int rc = join_side(c)) return rc;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  const char* p = static_cast<const char*>(buf) + sizeof(h);
+  for (const auto& b : ckpt_blocks(c)) {
+    CUDA_TRY(c, cudaMemcpyAsync(b.ptr, p, b.bytes, cudaMemcpyHostToDevice, c->stream));
+    p += b.bytes;
+  }
+  const unsigned long long cl = (unsigned long long)h.clamps;
+  const unsigned e = (unsigned)h.sticky;
+  CUDA_TRY(c, cudaMemcpyAsync(c->clamps, &cl, sizeof(cl), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->err, &e, sizeof(e), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));  // the host values above go out of scope
+  c->sticky = e;
+  c->f_state = h.f_state;
+  c->last_t = h.last_t;
+  c->have_particles = c->have_zones = true;
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------
  * Device memory of a context, and the lattice pool.
  * ------------------------------------------------------------------------- */
 static size_t round_alloc(size_t b) { return (b + 511) / 512 * 512; }
@@ -1237,13 +1368,11 @@ extern "C" int d3q19_pool_create(int device, int storage, int rebuild_freq, int 
   return 0;
 }
 
-extern "C" int d3q19_pool_admit(d3q19_pool* p, const int_param_struct* ip, const flp_param_struct* fp,
-                                const d3q19_options* opt, const float* f, const float* u, const float* tau,
-                                const float* parKin, const float* parForce, const float* parFluidForce,
-                                const float* spherePoints, const int* zoneNeighDat, const int* parsZone,
-                                const int* zoneMembers, const int* numParInZone, int* slot_out) {
-  if (!p || !ip || !fp || !f || !u || !slot_out) return D3Q19_EINVAL;
-  d3q19_options o;
+// Checks a member's parameters against the pool and finds it a slot and
+// budget: the options it is created with, the slot and its device bytes.
+static int pool_place(d3q19_pool* p, const int_param_struct* ip, const d3q19_options* opt, d3q19_options* out,
+                      int* slot, size_t* bytes) {
+  d3q19_options& o = *out;
   memset(&o, 0, sizeof(o));
   if (opt) o = *opt;
   o.device = p->dev;
@@ -1259,15 +1388,27 @@ extern "C" int d3q19_pool_admit(d3q19_pool* p, const int_param_struct* ip, const
     return pfail(p, D3Q19_EINVAL, "rebuild_freq %d differs from the pool's %d", o.rebuild_freq, p->rebuild);
   if (ip->NumParticles > 0 && ip->PointsPerWorkGroup > 256)
     return pfail(p, D3Q19_EINVAL, "PointsPerWorkGroup above 256");
-  int s = -1;
-  for (int k = 0; k < p->max_slots && s < 0; k++)
-    if (!p->slot[k]) s = k;
-  if (s < 0) return pfail(p, D3Q19_EBUSY, "all %d slots are taken", p->max_slots);
-  size_t bytes = 0;
-  if (int rc = d3q19_context_bytes(ip, &o, &bytes)) return rc;
-  if (p->used + bytes > p->budget)
-    return pfail(p, D3Q19_EBUSY, "%zu bytes would exceed the HBM budget (%zu of %zu used)", bytes, p->used,
+  *slot = -1;
+  for (int k = 0; k < p->max_slots && *slot < 0; k++)
+    if (!p->slot[k]) *slot = k;
+  if (*slot < 0) return pfail(p, D3Q19_EBUSY, "all %d slots are taken", p->max_slots);
+  if (int rc = d3q19_context_bytes(ip, &o, bytes)) return rc;
+  if (p->used + *bytes > p->budget)
+    return pfail(p, D3Q19_EBUSY, "%zu bytes would exceed the HBM budget (%zu of %zu used)", *bytes, p->used,
                  p->budget);
+  return 0;
+}
+
+extern "C" int d3q19_pool_admit(d3q19_pool* p, const int_param_struct* ip, const flp_param_struct* fp,
+                                const d3q19_options* opt, const float* f, const float* u, const float* tau,
+                                const float* parKin, const float* parForce, const float* parFluidForce,
+                                const float* spherePoints, const int* zoneNeighDat, const int* parsZone,
+                                const int* zoneMembers, const int* numParInZone, int* slot_out) {
+  if (!p || !ip || !fp || !f || !u || !slot_out) return D3Q19_EINVAL;
+  d3q19_options o;
+  int s = -1;
+  size_t bytes = 0;
+  if (int rc = pool_place(p, ip, opt, &o, &s, &bytes)) return rc;
   d3q19_ctx* c = nullptr;
   int rc = d3q19_create(ip, fp, &o, &c);
   if (rc) return pfail(p, rc, "%s", d3q19_last_error(nullptr));
@@ -1503,6 +1644,46 @@ extern "C" int d3q19_pool_release(d3q19_pool* p, int slot) {
   p->slot_bytes[slot] = 0;
   p->slot_steps[slot] = 0;
   p->dirty = true;
+  return 0;
+}
+
+extern "C" int d3q19_pool_evict(d3q19_pool* p, int slot, void* buf, size_t bytes) {
+  if (!p || slot < 0 || slot >= p->max_slots || !p->slot[slot]) return D3Q19_EINVAL;
+  cudaSetDevice(p->dev);
+  POOL_TRY(p, cudaStreamSynchronize(p->stream));
+  d3q19_ctx* c = p->slot[slot];
+  if (int rc = d3q19_checkpoint(c, buf, bytes)) return pfail(p, rc, "%s", d3q19_last_error(c));
+  return d3q19_pool_release(p, slot);
+}
+
+extern "C" int d3q19_pool_readmit(d3q19_pool* p, const int_param_struct* ip, const flp_param_struct* fp,
+                                  const d3q19_options* opt, const void* buf, size_t bytes, int* slot_out) {
+  if (!p || !ip || !fp || !buf || !slot_out) return D3Q19_EINVAL;
+  if (bytes < sizeof(CkptHeader)) return pfail(p, D3Q19_EINVAL, "not a checkpoint");
+  CkptHeader h;
+  memcpy(&h, buf, sizeof(h));
+  // A member leaves and rejoins between chunks, in the pool's phase.
+  if (h.f_state != 2 || h.last_t <= 0 || h.last_t % p->period != 0)
+    return pfail(p, D3Q19_EINVAL, "checkpoint at step %d is not at a step multiple of the period %d", h.last_t,
+                 p->period);
+  d3q19_options o;
+  int s = -1;
+  size_t need = 0;
+  if (int rc = pool_place(p, ip, opt, &o, &s, &need)) return rc;
+  d3q19_ctx* c = nullptr;
+  int rc = d3q19_create(ip, fp, &o, &c);
+  if (rc) return pfail(p, rc, "%s", d3q19_last_error(nullptr));
+  if ((rc = d3q19_restore(c, buf, bytes))) {
+    pfail(p, rc, "readmission: %s", d3q19_last_error(c));
+    d3q19_destroy(c);
+    return rc;
+  }
+  p->slot[s] = c;
+  p->slot_bytes[s] = need;
+  p->slot_steps[s] = h.last_t;
+  p->used += need;
+  p->dirty = true;
+  *slot_out = s;
   return 0;
 }
 

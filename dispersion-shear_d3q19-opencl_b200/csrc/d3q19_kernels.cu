@@ -683,7 +683,11 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
   }
 
   int nclamp = 0;
-#pragma unroll 1
+#ifndef FLUID_ZZ_UNROLL
+#define FLUID_ZZ_UNROLL 1
+#endif
+  constexpr int kZZUnroll = FLUID_ZZ_UNROLL;
+#pragma unroll kZZUnroll
   for (int zz = 0; zz < 2; zz++) {
     const int z = Z0 + 2 * threadIdx.z + zz;
     if (!inxy || z < 1 || z > g.Nz - 2) continue;

@@ -142,6 +142,12 @@ def cuda_lib():
         lib.d3q19_pool_last_error.argtypes = [P]
         lib.d3q19_pool_destroy.argtypes = [P]
         lib.d3q19_pool_mean_stress.argtypes = [P, P, P, P, P]
+        lib.d3q19_checkpoint_bytes.argtypes = [P, C.POINTER(C.c_size_t)]
+        lib.d3q19_checkpoint.argtypes = [P, P, C.c_size_t]
+        lib.d3q19_restore.argtypes = [P, P, C.c_size_t]
+        lib.d3q19_pool_evict.argtypes = [P, C.c_int, P, C.c_size_t]
+        lib.d3q19_pool_readmit.argtypes = [P, C.POINTER(IntParams), C.POINTER(FlpParams), C.POINTER(Options), P,
+                                           C.c_size_t, C.POINTER(C.c_int)]
         _cuda = lib
     return _cuda
 
@@ -399,6 +405,19 @@ class Simulation:
         self._check(self.lib.d3q19_mean_stress(self.h, C.byref(a), C.byref(b), C.byref(c)), "mean_stress")
         return a.value, b.value, c.value
 
+    def checkpoint(self) -> np.ndarray:
+        """The whole device state (d3q19_checkpoint) as a uint8 array."""
+        n = C.c_size_t()
+        self._check(self.lib.d3q19_checkpoint_bytes(self.h, C.byref(n)), "checkpoint_bytes")
+        buf = np.zeros(n.value, np.uint8)
+        self._check(self.lib.d3q19_checkpoint(self.h, _ptr(buf), buf.nbytes), "checkpoint")
+        return buf
+
+    def restore(self, buf):
+        """Loads a checkpoint of a context with the same parameters."""
+        b = np.ascontiguousarray(buf, np.uint8)
+        self._check(self.lib.d3q19_restore(self.h, _ptr(b), b.nbytes), "restore")
+
     def profile(self, enable: bool):
         self._check(self.lib.d3q19_profile(self.h, int(enable)), "profile")
 
@@ -518,6 +537,32 @@ class Pool:
     def steps(self, slot: int) -> int:
         return int(self.lib.d3q19_pool_slot_steps(self.h, slot))
 
+    def evict(self, slot: int):
+        """Checkpoints the member and frees its slot; returns (checkpoint,
+        parameters) for readmit."""
+        n = C.c_size_t()
+        hnd = self.lib.d3q19_pool_context(self.h, slot)
+        if not hnd:
+            raise D3Q19Error(f"pool slot {slot} is free")
+        self._check(self.lib.d3q19_checkpoint_bytes(C.c_void_p(hnd), C.byref(n)), "checkpoint_bytes")
+        buf = np.zeros(n.value, np.uint8)
+        self._check(self.lib.d3q19_pool_evict(self.h, slot, _ptr(buf), buf.nbytes), "pool_evict")
+        return buf, self.members.pop(slot)
+
+    def readmit(self, evicted):
+        """Re-admits an evicted member; returns its slot, or None when the
+        pool has no room for it now (EBUSY)."""
+        buf, (ip, fp, opt) = evicted
+        b = np.ascontiguousarray(buf, np.uint8)
+        slot = C.c_int(-1)
+        rc = self.lib.d3q19_pool_readmit(self.h, C.byref(ip), C.byref(fp), C.byref(opt), _ptr(b), b.nbytes,
+                                         C.byref(slot))
+        if rc == EBUSY:
+            return None
+        self._check(rc, "pool_readmit")
+        self.members[slot.value] = (ip, fp, opt)
+        return slot.value
+
     def release(self, slot: int):
         self._check(self.lib.d3q19_pool_release(self.h, slot), "pool_release")
         self.members.pop(slot, None)
@@ -546,12 +591,6 @@ class Pool:
         if getattr(self, "h", None):
             self.lib.d3q19_pool_destroy(self.h)
             self.h = None
-
-    def __del__(self):
-        try:
-            self.close()
-        except Exception:
-            pass
 
     def __del__(self):
         try:

@@ -11,9 +11,12 @@ until `max_steps`.
 The server admits requests as they arrive, as long as a slot and HBM budget
 are free; every member of the pool advances in the same batched launches, so
 requests that arrive while others run overlap with them on the device, and a
-finished request frees its memory for the queue.  The reference has no
-counterpart (one lattice per process); the physics of each request is the
-reference's.
+finished request frees its memory for the queue.  With pre-emption on, a
+request that does not fit may evict a long-running member (its checkpoint
+goes to host memory, d3q19_pool_evict); the evicted member is re-admitted
+(d3q19_pool_readmit) ahead of every request that arrived after its eviction
+and continues bit for bit.  The reference has no counterpart (one lattice per
+process); the physics of each request is the reference's.
 """
 from __future__ import annotations
 
@@ -113,6 +116,7 @@ class SolveRecord:
     eff_viscosity: float
     converged: bool
     failed: bool = False  # the solve stopped on a device error (non-finite state)
+    preempted: int = 0    # times the solve was evicted and re-admitted
 
     @property
     def latency(self) -> float:
@@ -141,7 +145,17 @@ def summary(records: list, wall: float) -> dict:
             "p99_latency_s": float(np.percentile(lat, 99)) if len(lat) else None,
             "converged": int(sum(r.converged for r in records)),
             "failed": int(sum(r.failed for r in records)),
+            "preempted": int(sum(r.preempted for r in records)),
             "steps": int(sum(r.steps for r in records))}
+
+
+@dataclasses.dataclass
+class _Member:
+    req: ShearRequest
+    start: float
+    conv: Convergence
+    base: int = 0        # pool step count at the (re)admission
+    preempted: int = 0
 
 
 class Server:
@@ -149,12 +163,20 @@ class Server:
     budget last, advance every member `check_every` steps at a time, retire
     the converged ones.  The host-side set-up of an arrived request (input
     parsing, sphere placement, initial state) runs on `builders` worker
-    threads while the GPU works."""
+    threads while the GPU works.
+
+    preempt_after: None (off) or a step count.  When the request at the head
+    of the queue does not fit, the member with the most steps since its
+    (re)admission is evicted if that count is at least preempt_after, and
+    again until the request fits or no member qualifies.  An evicted member
+    is re-admitted before any request that arrived after its eviction."""
 
     def __init__(self, pool: Pool, check_every: int = 500, rel_tol: float = 1e-4, max_steps: int = 20000,
-                 clock=time.perf_counter, sleep=time.sleep, builders: int = 4):
+                 clock=time.perf_counter, sleep=time.sleep, builders: int = 4, preempt_after: int | None = None):
         if check_every % pool.period:
             raise ValueError(f"check_every must be a multiple of the pool period {pool.period}")
+        if preempt_after is not None and preempt_after <= 0:
+            raise ValueError("preempt_after must be positive")
         self.pool = pool
         self.check_every = check_every
         self.rel_tol = rel_tol
@@ -162,6 +184,7 @@ class Server:
         self.clock = clock
         self.sleep = sleep
         self.builders = builders
+        self.preempt_after = preempt_after
 
     def _stresses(self, active):
         """{slot: (stress, viscosity) or None for a failed member}."""
@@ -184,8 +207,9 @@ class Server:
         (records in completion order, wall seconds)."""
         queue = sorted(requests, key=lambda r: r.arrival)
         t0 = self.clock()
-        active = {}  # slot -> (request, start time, Convergence)
+        active = {}   # slot -> _Member
         joining = {}  # admitted while the pool was running: join the next chunk
+        parked = []   # (queue index it waits for, _Member, checkpoint) in eviction order
         done = []
         ex = ThreadPoolExecutor(max_workers=self.builders) if self.builders > 0 else None
         built = {}  # rid -> Future or host state of an arrived request
@@ -200,11 +224,40 @@ class Server:
                 built[req.rid] = ex.submit(build, req) if ex else build(req)
                 nb += 1
 
-        def admit_arrived():
-            # Admit in arrival order; stop at the first one that does not fit.
+        def evict_one():
+            # The member with the most steps since its (re)admission, if it
+            # has run at least preempt_after of them.
+            if self.preempt_after is None:
+                return False
+            best, run = None, -1
+            for slot, m in active.items():
+                n = self.pool.steps(slot) - m.base
+                if n >= self.preempt_after and n > run:
+                    best, run = slot, n
+            if best is None:
+                return False
+            m = active.pop(best)
+            m.preempted += 1
+            parked.append((nb, m, self.pool.evict(best)))
+            return True
+
+        def admit_arrived(preempt):
+            # Parked members that are due first, then arrivals in order; stop
+            # at the first one that does not fit.
             nonlocal qi
             prepare()
-            while qi < nb:
+            while True:
+                if parked and parked[0][0] <= qi:
+                    _, m, ck = parked[0]
+                    slot = self.pool.readmit(ck)
+                    if slot is None:
+                        return
+                    parked.pop(0)
+                    m.base = self.pool.steps(slot)
+                    joining[slot] = m
+                    continue
+                if qi >= nb:
+                    return
                 req = queue[qi]
                 hs = built[req.rid]
                 if ex:
@@ -212,44 +265,48 @@ class Server:
                 slot = self.pool.admit(hs)
                 if slot is None:
                     built[req.rid] = hs if not ex else _done_future(hs)
+                    if preempt and evict_one():
+                        continue
                     if not active and not joining:
                         raise RuntimeError(f"request {req.rid} does not fit an empty pool")
                     return
                 del built[req.rid]
-                joining[slot] = (req, self.clock() - t0, Convergence(self.rel_tol))
+                joining[slot] = _Member(req, self.clock() - t0, Convergence(self.rel_tol), self.pool.steps(slot))
                 qi += 1
 
         try:
-            while qi < len(queue) or active or joining:
-                admit_arrived()
+            while qi < len(queue) or active or joining or parked:
+                admit_arrived(True)
                 active.update(joining)
                 joining.clear()
                 if not active:
-                    self.sleep(max(0.0, queue[qi].arrival - (self.clock() - t0)))
+                    if qi < len(queue):
+                        self.sleep(max(0.0, queue[qi].arrival - (self.clock() - t0)))
                     continue
                 # The chunk runs on the pool's stream while the host admits the
                 # requests that arrived meanwhile (their set-up and first steps
                 # overlap the chunk on the device); they join the next chunk.
                 self.pool.advance(self.check_every)
-                admit_arrived()
+                admit_arrived(False)
                 stresses = self._stresses(active)
                 for slot in list(active):
-                    req, start, conv = active[slot]
+                    m = active[slot]
+                    req = m.req
                     steps = self.pool.steps(slot)
                     res = stresses[slot]
                     if res is None:
                         # A member whose state went non-finite retires as failed;
                         # the others are independent of it.
-                        done.append(SolveRecord(req.rid, req.arrival, start, self.clock() - t0, steps, float("nan"),
-                                                float("nan"), False, True))
+                        done.append(SolveRecord(req.rid, req.arrival, m.start, self.clock() - t0, steps,
+                                                float("nan"), float("nan"), False, True, m.preempted))
                         self.pool.release(slot)
                         del active[slot]
                         continue
                     stress, visc = res
-                    ok = conv.update(stress)
+                    ok = m.conv.update(stress)
                     if ok or steps >= self.max_steps:
-                        done.append(SolveRecord(req.rid, req.arrival, start, self.clock() - t0, steps, stress, visc,
-                                                ok))
+                        done.append(SolveRecord(req.rid, req.arrival, m.start, self.clock() - t0, steps, stress,
+                                                visc, ok, False, m.preempted))
                         self.pool.release(slot)
                         del active[slot]
         finally:

@@ -288,6 +288,21 @@ void* d3q19_stream(d3q19_ctx* ctx);
  * ctx is NULL). */
 const char* d3q19_last_error(d3q19_ctx* ctx);
 
+/* Checkpoints (no counterpart in the reference, which writes text output
+ * only): the whole device state of a context -- the distributions the next
+ * step reads, u, the local tau, the sphere state and partial sums, the marker
+ * records and tile lists of the last particle pass, the zone lists, the step
+ * number and the clamp counter -- in one host buffer of
+ * d3q19_checkpoint_bytes bytes.  d3q19_restore loads it into a context
+ * created with the same parameter blocks and options; the steps after it are
+ * bit-identical to those of the context it came from.  A context with a
+ * device error, or left between passes by d3q19_k_*, is not checkpointed
+ * (D3Q19_ENUMERIC / D3Q19_EOVERFLOW / D3Q19_ESTATE); a buffer of another
+ * lattice, sphere count or option set is refused with D3Q19_EINVAL. */
+int d3q19_checkpoint_bytes(d3q19_ctx* ctx, size_t* bytes);
+int d3q19_checkpoint(d3q19_ctx* ctx, void* buf, size_t bytes);
+int d3q19_restore(d3q19_ctx* ctx, const void* buf, size_t bytes);
+
 /* Replaces clRelease* (sim_main.c:503-525). */
 int d3q19_destroy(d3q19_ctx* ctx);
 
@@ -342,6 +357,15 @@ int d3q19_pool_mean_stress(d3q19_pool* pool, double* stress_xz, double* shear_ra
                            int* status);
 /* Frees the member's slot and device memory. */
 int d3q19_pool_release(d3q19_pool* pool, int slot);
+/* Pre-emption: d3q19_pool_evict writes the member's checkpoint to buf
+ * (d3q19_checkpoint_bytes of d3q19_pool_context(slot)) and releases the
+ * slot; d3q19_pool_readmit creates a member from the same parameter blocks
+ * and options and the checkpoint, and continues it from its step (no warm-up
+ * steps) in the next advance.  Results equal those of a member that was
+ * never evicted.  EBUSY as for d3q19_pool_admit. */
+int d3q19_pool_evict(d3q19_pool* pool, int slot, void* buf, size_t bytes);
+int d3q19_pool_readmit(d3q19_pool* pool, const int_param_struct* ip, const flp_param_struct* fp,
+                       const d3q19_options* opt, const void* buf, size_t bytes, int* slot_out);
 /* Budget in use, the budget, and the member count. */
 int d3q19_pool_usage(d3q19_pool* pool, size_t* used, size_t* budget, int* members);
 /* Persistent grid sizes (CTAs) of the batched fluid, particle and contact

@@ -48,7 +48,7 @@ class FakeMember:
     def mean_stress(self):
         s = self.pool.steps_done[self.slot]
         # Relaxes towards the target: converges after a request-dependent time.
-        return self.target * (1.0 - np.exp(-s / 1000.0)), 0.0, 0.0
+        return self.target * (1.0 - np.exp(-s / self.pool.tconst.get(self.slot, 1000.0))), 0.0, 0.0
 
 
 class FakePool:
@@ -56,20 +56,45 @@ class FakePool:
 
     def __init__(self, budget):
         self.budget, self.used = budget, 0
-        self.steps_done, self.size, self.target = {}, {}, {}
+        self.steps_done, self.size, self.target, self.tconst, self.rid = {}, {}, {}, {}, {}
         self.admitted, self.max_members, self.next = [], 0, 0
+        self.evicted, self.readmitted = [], []
+        self.events, self.now = [], lambda: 0.0  # (kind, rid, time) in call order
 
-    def admit(self, hs):
+    def admit(self, hs, steps=None):
         b = hs["bytes"]
         if self.used + b > self.budget:
             return None
         s = self.next
         self.next += 1
         self.used += b
-        self.size[s], self.steps_done[s], self.target[s] = b, self.period, hs["target"]
-        self.admitted.append(hs["rid"])
+        self.size[s], self.target[s] = b, hs["target"]
+        self.steps_done[s] = self.period if steps is None else steps
+        self.tconst[s] = hs.get("tconst", 1000.0)
+        self.rid[s] = hs["rid"]
+        if steps is None:
+            self.admitted.append(hs["rid"])
+            self.events.append(("admit", hs["rid"], self.now()))
         self.max_members = max(self.max_members, len(self.size))
         return s
+
+    # Checkpoints hold the member's state: its step count and parameters.
+    def evict(self, s):
+        assert self.steps_done[s] % self.period == 0
+        ck = ({"bytes": self.size[s], "rid": self.rid[s], "target": self.target[s], "tconst": self.tconst[s]},
+              self.steps_done[s])
+        self.evicted.append(ck[0]["rid"])
+        self.events.append(("evict", ck[0]["rid"], self.now()))
+        self.release(s)
+        return ck
+
+    def readmit(self, ck):
+        slot = self.admit(ck[0], steps=ck[1])
+        if slot is not None:
+            self.readmitted.append(ck[0]["rid"])
+            self.events.append(("readmit", ck[0]["rid"], self.now()))
+        return slot
+
 
     def advance(self, n):
         for s in self.size:
@@ -83,6 +108,7 @@ class FakePool:
 
     def release(self, s):
         self.used -= self.size.pop(s)
+
 
 
 def test_server_admits_in_order_within_budget_and_retires():
@@ -143,3 +169,72 @@ def test_server_retires_a_failed_member_and_goes_on():
     by = {r.rid: r for r in recs}
     assert by[1].failed and not by[1].converged and by[0].converged and by[2].converged
     assert sv.summary(recs, 1.0)["failed"] == 1 and pool.used == 0
+
+
+def serve_long_then_short(preempt_after):
+    # One slot's worth of budget; a long solve arrives first, three short ones
+    # just after it.
+    reqs = [sv.ShearRequest(rid=i, edge=(32, 32, 32), phi=0.0, model="newtonian", wall_speed=0.02, seed=1,
+                            arrival=1e-3 * i) for i in range(4)]
+    pool = FakePool(budget=10)
+    clock = {"t": 0.0}
+
+    def now():
+        clock["t"] += 1e-4
+        return clock["t"]
+
+    build = lambda r: {"bytes": 10, "rid": r.rid, "target": 1.0, "tconst": 4000.0 if r.rid == 0 else 200.0}
+    srv = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=60000, clock=now,
+                    sleep=lambda dt: clock.__setitem__("t", clock["t"] + dt), builders=0,
+                    preempt_after=preempt_after)
+    recs, wall = srv.run(reqs, build=build)
+    return {r.rid: r for r in recs}, pool
+
+
+def test_preemption_lets_short_solves_past_a_long_one():
+    plain, pool0 = serve_long_then_short(None)
+    pre, pool1 = serve_long_then_short(3000)
+    assert pool0.evicted == [] and [r.rid for r in sorted(plain.values(), key=lambda r: r.finish)] == [0, 1, 2, 3]
+    # With pre-emption the long solve is evicted (checkpointed) once the short
+    # ones wait, and finishes last.
+    assert pool1.evicted and set(pool1.evicted) == {0} and pool1.readmitted == pool1.evicted
+    assert max(pre.values(), key=lambda r: r.finish).rid == 0 and pre[0].preempted == len(pool1.evicted)
+    # Every solve takes the same steps either way (it continues from its
+    # checkpoint), the short ones finish earlier, and the pool ends empty.
+    assert all(pre[i].steps == plain[i].steps and pre[i].converged for i in range(4))
+    assert all(pre[i].finish < plain[i].finish for i in (1, 2, 3))
+    assert pool1.used == 0 and sv.summary(list(pre.values()), 1.0)["preempted"] == pre[0].preempted
+
+
+def test_preempted_member_is_not_starved():
+    # Arrivals keep coming: an evicted member is re-admitted before every
+    # request that arrived after its eviction.
+    reqs = [sv.ShearRequest(rid=i, edge=(32, 32, 32), phi=0.0, model="newtonian", wall_speed=0.02, seed=1,
+                            arrival=0.0 if i == 0 else 0.004 * i) for i in range(12)]
+    arrival = {r.rid: r.arrival for r in reqs}
+    pool = FakePool(budget=20)
+    clock = {"t": 0.0}
+
+    def now():
+        clock["t"] += 1e-3
+        return clock["t"]
+
+    pool.now = lambda: clock["t"]
+    build = lambda r: {"bytes": 10, "rid": r.rid, "target": 1.0, "tconst": 3000.0 if r.rid % 4 == 0 else 400.0}
+    recs, _ = sv.Server(pool, check_every=500, max_steps=60000, clock=now,
+                        sleep=lambda dt: clock.__setitem__("t", clock["t"] + dt), builders=0,
+                        preempt_after=1000).run(reqs, build=build)
+    assert sorted(r.rid for r in recs) == list(range(12)) and all(r.converged for r in recs)
+    assert pool.evicted and sorted(pool.readmitted) == sorted(pool.evicted) and pool.used == 0
+    ev = pool.events
+    for i, (kind, rid, te) in enumerate(ev):
+        if kind != "evict":
+            continue
+        j = next(k for k in range(i + 1, len(ev)) if ev[k][:2] == ("readmit", rid))
+        # Admitted while it waited: only requests that had arrived by its eviction.
+        assert all(arrival[r] <= te for kd, r, _ in ev[i + 1:j] if kd == "admit")
+
+
+def test_preempt_after_must_be_positive():
+    with pytest.raises(ValueError):
+        sv.Server(FakePool(10), check_every=500, preempt_after=0)
