@@ -559,6 +559,71 @@ def run_served(args):
                                                                "median": float(np.median(visc_err))}}
 
 
+def run_served_preempt(args):
+    """cfg: the served sweep's Poisson arrivals (50/s, seeded) on an FP16 pool
+    whose HBM budget holds a few members at a time, served twice: admission
+    in arrival order only, and with pre-emption (a request that does not fit
+    evicts the member with the most steps since its admission, once that is
+    at least 2000; the evicted member's checkpoint waits in host memory and
+    is re-admitted before later arrivals).  Reports throughput, latency and
+    the measured cost of the evictions and re-admissions."""
+    import numpy as np
+    import torch
+
+    import d3q19_b200 as d3
+    from d3q19_b200 import serving as sv
+
+    torch.cuda.set_device(0)
+    reqs = sv.make_requests(args.requests, 50.0, 2025, edges=(32, 64))
+    max_steps = 40000
+    budget = 160 << 20
+    out = {}
+    for label, pre in (("arrival_order", None), ("preempt_2000", 2000)):
+        pool = d3.Pool(storage=1, max_slots=64, hbm_budget=budget)
+        cost = {"evict_s": 0.0, "readmit_s": 0.0, "bytes": 0, "n": 0}
+        ev, re = pool.evict, pool.readmit
+
+        def evict(slot, ev=ev, cost=cost):
+            t = time.perf_counter()
+            r = ev(slot)
+            cost["evict_s"] += time.perf_counter() - t
+            cost["bytes"] += int(r[0].nbytes)
+            cost["n"] += 1
+            return r
+
+        def readmit(ck, re=re, cost=cost):
+            t = time.perf_counter()
+            r = re(ck)
+            cost["readmit_s"] += time.perf_counter() - t
+            return r
+
+        pool.evict, pool.readmit = evict, readmit
+        recs, wall = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=max_steps, preempt_after=pre).run(reqs)
+        pool.close()
+        summ = sv.summary(recs, wall)
+        summ["evictions"] = cost["n"]
+        summ["checkpoint_mb_total"] = round(cost["bytes"] / 1e6, 1)
+        summ["evict_s_total"] = round(cost["evict_s"], 3)
+        summ["readmit_s_total"] = round(cost["readmit_s"], 3)
+        summ["latency_by_rid"] = {r.rid: round(r.latency, 3) for r in recs}
+        out[label] = summ
+    a, b = out["arrival_order"], out["preempt_2000"]
+    lat_a = np.array([a["latency_by_rid"][r.rid] for r in reqs])
+    lat_b = np.array([b["latency_by_rid"][r.rid] for r in reqs])
+    for v in out.values():
+        del v["latency_by_rid"]
+    return {"metric": "solves/s (served sweep, HBM-limited pool)", "value": round(b["solves_per_s"], 3),
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32 arithmetic, f16 shifted storage", "data": "synthetic (seeded Poisson arrivals)",
+            "impl": "ours",
+            "config": {"workload": "served-preempt", "requests": len(reqs), "arrival_rate_per_s": 50.0,
+                       "edges": [32, 64], "phi": [0.0, 0.3], "models": list(sv.MODELS), "hbm_budget_mb": budget >> 20,
+                       "stop": "1e-4 over 500 steps", "max_steps": max_steps},
+            "runs": out,
+            "requests_faster_with_preemption": int(np.sum(lat_b < lat_a)),
+            "median_latency_ratio_preempt_over_arrival_order": round(float(np.median(lat_b / lat_a)), 3)}
+
+
 def run_precision(args):
     """Casson suspension: 256x128x256 lattice, 1000 spheres of radius 6 (384
     markers each, seeded random placement), regularised Casson yield stress
@@ -630,6 +695,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dense-powerlaw-128", choices=sorted(WORKLOADS) + ["batch-64",
                                                                                            "served-sweep",
+                                                                                           "served-preempt",
                                                                                            "casson-precision"])
     ap.add_argument("--requests", type=int, default=128, help="served-sweep: number of requests")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -645,9 +711,10 @@ def main():
         if rank == 0:
             print(json.dumps(run_reference_arm(args)), flush=True)
         return
-    if args.workload in ("batch-64", "served-sweep", "casson-precision"):
+    if args.workload in ("batch-64", "served-sweep", "served-preempt", "casson-precision"):
         if rank == 0:
-            run = {"batch-64": run_batch, "served-sweep": run_served, "casson-precision": run_precision}
+            run = {"batch-64": run_batch, "served-sweep": run_served, "served-preempt": run_served_preempt,
+                   "casson-precision": run_precision}
             print(json.dumps(run[args.workload](args)), flush=True)
         return
     dist = None
