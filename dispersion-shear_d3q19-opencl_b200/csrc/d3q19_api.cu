@@ -78,6 +78,12 @@ struct d3q19_ctx {
   size_t scratch_bytes = 0;
   bool have_particles = false, have_zones = false;
   unsigned sticky = 0;
+  // A member of a lattice pool takes its device memory from the pool's
+  // stream-ordered memory pool (allocated on its own stream); its release
+  // frees it in the order of free_stream, after the pool's work in flight,
+  // without waiting for the device.
+  cudaMemPool_t mempool = nullptr;
+  cudaStream_t free_stream = nullptr;
   std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;
   bool profiling = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_fluid, ev_part;
@@ -103,10 +109,20 @@ static int fail(d3q19_ctx* c, int code, const char* fmt, ...) {
     if (e_ != cudaSuccess) return fail((c), D3Q19_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
   } while (0)
 
+static cudaError_t dev_alloc(d3q19_ctx* c, void** p, size_t bytes) {
+  return c->mempool ? cudaMallocFromPoolAsync(p, bytes, c->mempool, c->stream) : cudaMalloc(p, bytes);
+}
+
+static void dev_free(d3q19_ctx* c, void* p) {
+  if (!p) return;
+  if (c->mempool) cudaFreeAsync(p, c->free_stream ? c->free_stream : c->stream);
+  else cudaFree(p);
+}
+
 template <typename T>
 static int dalloc(d3q19_ctx* c, T** p, size_t n) {
   if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  cudaError_t e = dev_alloc(c, (void**)p, n * sizeof(T));
   if (e != cudaSuccess) {
     *p = nullptr;
     return fail(c, D3Q19_ENOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
@@ -184,8 +200,16 @@ static int validate(const int_param_struct* ip, const flp_param_struct* fp, cons
   return 0;
 }
 
+static int create_ctx(const int_param_struct* ip, const flp_param_struct* fp, const d3q19_options* opt,
+                      cudaMemPool_t mempool, d3q19_ctx** out);
+
 extern "C" int d3q19_create(const int_param_struct* ip, const flp_param_struct* fp, const d3q19_options* opt,
                             d3q19_ctx** out) {
+  return create_ctx(ip, fp, opt, nullptr, out);
+}
+
+static int create_ctx(const int_param_struct* ip, const flp_param_struct* fp, const d3q19_options* opt,
+                      cudaMemPool_t mempool, d3q19_ctx** out) {
   if (!ip || !fp || !out) return fail(nullptr, D3Q19_EINVAL, "null argument");
   d3q19_options o;
   memset(&o, 0, sizeof(o));
@@ -209,6 +233,7 @@ extern "C" int d3q19_create(const int_param_struct* ip, const flp_param_struct* 
   c->fp = *fp;
   c->opt = o;
   c->dev = o.device;
+  c->mempool = mempool;
   cudaSetDevice(c->dev);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
@@ -816,10 +841,10 @@ extern "C" int d3q19_read_parfluidforce(d3q19_ctx* c, float* k) {
 
 static int ensure_scratch(d3q19_ctx* c, size_t bytes) {
   if (c->scratch_bytes >= bytes) return 0;
-  if (c->scratch) cudaFree(c->scratch);
+  dev_free(c, c->scratch);
   c->scratch = nullptr;
   c->scratch_bytes = 0;
-  CUDA_TRY(c, cudaMalloc(&c->scratch, bytes));
+  CUDA_TRY(c, dev_alloc(c, &c->scratch, bytes));
   c->scratch_bytes = bytes;
   return 0;
 }
@@ -1020,8 +1045,7 @@ extern "C" int d3q19_destroy(d3q19_ctx* c) {
                   c->sphere, c->mrec, c->tile_count, c->fmax, c->tile_list, c->znd, c->parsZone, c->zoneMembers,
                   c->numParInZone, c->revStart, c->revList, c->zoneOf, c->err, c->clamps, c->pstats, c->scratch,
                   c->tau64, c->kin64[0], c->kin64[1], c->pff64[0], c->pff64[1]};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  for (void* p : ptrs) dev_free(c, p);
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->side) cudaStreamDestroy(c->side);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -1281,6 +1305,10 @@ struct d3q19_pool {
   size_t budget = 0, used = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_done = nullptr;
+  // Device memory of the members: allocated on a member's stream at
+  // admission, freed on the pool's stream at release (after the chunks in
+  // flight), kept reserved between members.
+  cudaMemPool_t mempool = nullptr;
   std::vector<d3q19_ctx*> slot;  // nullptr: free
   std::vector<size_t> slot_bytes;
   std::vector<long long> slot_steps;
@@ -1352,8 +1380,16 @@ extern "C" int d3q19_pool_create(int device, int storage, int rebuild_freq, int 
   p->fblocks = pr.multiProcessorCount * (storage == STORE_F32 ? 5 : 4);
   p->pblocks = pr.multiProcessorCount * 4;
   p->cblocks = pr.multiProcessorCount * 4;
+  cudaMemPoolProps mp;
+  memset(&mp, 0, sizeof(mp));
+  mp.allocType = cudaMemAllocationTypePinned;
+  mp.location.type = cudaMemLocationTypeDevice;
+  mp.location.id = device;
+  const unsigned long long keep = ~0ull;
   if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&p->ev_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMemPoolCreate(&p->mempool, &mp) != cudaSuccess ||
+      cudaMemPoolSetAttribute(p->mempool, cudaMemPoolAttrReleaseThreshold, (void*)&keep) != cudaSuccess ||
       cudaMalloc(&p->d_fargs, sizeof(FluidArgs) * 2 * max_slots) != cudaSuccess ||
       cudaMalloc(&p->d_pargs, sizeof(ParticleArgs) * 2 * max_slots) != cudaSuccess ||
       cudaMalloc(&p->d_zargs, sizeof(ZoneArgs) * 2 * max_slots) != cudaSuccess ||
@@ -1410,7 +1446,7 @@ extern "C" int d3q19_pool_admit(d3q19_pool* p, const int_param_struct* ip, const
   size_t bytes = 0;
   if (int rc = pool_place(p, ip, opt, &o, &s, &bytes)) return rc;
   d3q19_ctx* c = nullptr;
-  int rc = d3q19_create(ip, fp, &o, &c);
+  int rc = create_ctx(ip, fp, &o, p->mempool, &c);
   if (rc) return pfail(p, rc, "%s", d3q19_last_error(nullptr));
   rc = d3q19_write_lattice(c, f, u, tau);
   if (!rc && ip->NumParticles > 0) {
@@ -1637,8 +1673,11 @@ extern "C" long long d3q19_pool_slot_steps(d3q19_pool* p, int slot) {
 extern "C" int d3q19_pool_release(d3q19_pool* p, int slot) {
   if (!p || slot < 0 || slot >= p->max_slots || !p->slot[slot]) return D3Q19_EINVAL;
   cudaSetDevice(p->dev);
-  POOL_TRY(p, cudaStreamSynchronize(p->stream));
-  d3q19_destroy(p->slot[slot]);
+  // No wait for the chunks in flight: the member's memory is freed in the
+  // pool stream's order, after them (its own streams are drained by destroy).
+  d3q19_ctx* c = p->slot[slot];
+  c->free_stream = p->stream;
+  d3q19_destroy(c);
   p->slot[slot] = nullptr;
   p->used -= p->slot_bytes[slot];
   p->slot_bytes[slot] = 0;
@@ -1671,7 +1710,7 @@ extern "C" int d3q19_pool_readmit(d3q19_pool* p, const int_param_struct* ip, con
   size_t need = 0;
   if (int rc = pool_place(p, ip, opt, &o, &s, &need)) return rc;
   d3q19_ctx* c = nullptr;
-  int rc = d3q19_create(ip, fp, &o, &c);
+  int rc = create_ctx(ip, fp, &o, p->mempool, &c);
   if (rc) return pfail(p, rc, "%s", d3q19_last_error(nullptr));
   if ((rc = d3q19_restore(c, buf, bytes))) {
     pfail(p, rc, "readmission: %s", d3q19_last_error(c));
@@ -1735,12 +1774,15 @@ extern "C" int d3q19_pool_destroy(d3q19_pool* p) {
   pool_drop_graphs(p);
   for (auto*& c : p->slot)
     if (c) {
+      c->free_stream = p->stream;
       d3q19_destroy(c);
       c = nullptr;
     }
   void* ptrs[] = {p->d_fargs, p->d_pargs, p->d_zargs, p->d_work, p->d_zslots, p->d_counts, p->d_stats};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  if (p->stream) cudaStreamSynchronize(p->stream);  // the members' stream-ordered frees
+  if (p->mempool) cudaMemPoolDestroy(p->mempool);
   if (p->ev_done) cudaEventDestroy(p->ev_done);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;

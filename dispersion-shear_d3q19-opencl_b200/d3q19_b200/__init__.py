@@ -513,6 +513,17 @@ class Pool:
                                     FlpParams.from_buffer_copy(bytes(hs.cfg.fp)), opt)
         return slot.value
 
+    def fits(self, hs: "HostState", **option_overrides) -> bool:
+        """Whether admit would find a slot and budget for the HostState now
+        (host arithmetic only)."""
+        opt = Options.from_buffer_copy(bytes(hs.options))
+        opt.storage = self.storage
+        opt.rebuild_freq = self.rebuild_freq
+        for k, v in option_overrides.items():
+            setattr(opt, k, v)
+        used, budget, n = self.usage()
+        return n < self.max_slots and used + context_bytes(hs.cfg.ip, opt) <= budget
+
     def advance(self, nsteps: int):
         self._check(self.lib.d3q19_pool_advance(self.h, nsteps), "pool_advance")
 

@@ -241,7 +241,22 @@ class Server:
             parked.append((nb, m, self.pool.evict(best)))
             return True
 
-        def admit_arrived(preempt):
+        def make_room():
+            # At a chunk boundary: while the request at the head of the queue
+            # has arrived and does not fit, evict a long runner.  The request
+            # is admitted while the next chunk runs.
+            prepare()
+            if self.preempt_after is None or qi >= nb or (parked and parked[0][0] <= qi):
+                return
+            req = queue[qi]
+            hs = built[req.rid]
+            if ex:
+                hs = hs.result()
+                built[req.rid] = _done_future(hs)
+            while not self.pool.fits(hs) and evict_one():
+                pass
+
+        def admit_arrived():
             # Parked members that are due first, then arrivals in order; stop
             # at the first one that does not fit.
             nonlocal qi
@@ -265,8 +280,6 @@ class Server:
                 slot = self.pool.admit(hs)
                 if slot is None:
                     built[req.rid] = hs if not ex else _done_future(hs)
-                    if preempt and evict_one():
-                        continue
                     if not active and not joining:
                         raise RuntimeError(f"request {req.rid} does not fit an empty pool")
                     return
@@ -276,7 +289,14 @@ class Server:
 
         try:
             while qi < len(queue) or active or joining or parked:
-                admit_arrived(True)
+                # Between chunks the GPU waits for the host, so requests are
+                # admitted here only into an empty pool; otherwise they are
+                # admitted while the next chunk runs.  Evictions need the
+                # members' state at a chunk boundary: they happen here.
+                if active or joining:
+                    make_room()
+                else:
+                    admit_arrived()
                 active.update(joining)
                 joining.clear()
                 if not active:
@@ -287,7 +307,7 @@ class Server:
                 # requests that arrived meanwhile (their set-up and first steps
                 # overlap the chunk on the device); they join the next chunk.
                 self.pool.advance(self.check_every)
-                admit_arrived(False)
+                admit_arrived()
                 stresses = self._stresses(active)
                 for slot in list(active):
                     m = active[slot]

@@ -69,6 +69,28 @@ def test_members_identical_alone_and_in_the_mix(storage):
     bits_equal(mixed[3], alone(REQS[3], storage, [100, 100]))
 
 
+def test_release_in_flight_and_memory_reuse():
+    # A release returns without waiting for the chunk in flight (the member's
+    # memory is freed in the pool stream's order); a member admitted right
+    # after it may reuse that memory.  Neither the member that stays nor the
+    # newcomer sees the difference.
+    pool = d3.Pool(storage=0, max_slots=4)
+    s0 = pool.admit(sv.host_state(REQS[0]))
+    s1 = pool.admit(sv.host_state(REQS[1]))
+    pool.advance(100)
+    pool.release(s1)  # the 100-step chunk is still queued or running
+    s2 = pool.admit(sv.host_state(REQS[2]))
+    pool.advance(100)
+    pool.release(s0)
+    s3 = pool.admit(sv.host_state(REQS[3]))
+    pool.advance(100)
+    got = {0: None, 2: state(pool, s2), 3: state(pool, s3)}
+    assert pool.steps(s2) == pool.period + 200 and pool.steps(s3) == pool.period + 100
+    pool.close()
+    bits_equal(got[2], alone(REQS[2], 0, [100, 100]))
+    bits_equal(got[3], alone(REQS[3], 0, [100]))
+
+
 @pytest.mark.parametrize("rid", [0, 1, 2])
 def test_member_matches_its_own_context(rid):
     req = REQS[rid]

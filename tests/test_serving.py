@@ -78,6 +78,9 @@ class FakePool:
         self.max_members = max(self.max_members, len(self.size))
         return s
 
+    def fits(self, hs):
+        return self.used + hs["bytes"] <= self.budget
+
     # Checkpoints hold the member's state: its step count and parameters.
     def evict(self, s):
         assert self.steps_done[s] % self.period == 0
