@@ -355,7 +355,9 @@ long long d3q19_pool_slot_steps(d3q19_pool* pool, int slot);
  * for a free slot (values NaN). */
 int d3q19_pool_mean_stress(d3q19_pool* pool, double* stress_xz, double* shear_rate, double* eff_viscosity,
                            int* status);
-/* Frees the member's slot and device memory. */
+/* Frees the member's slot and device memory.  Returns without waiting for
+ * the pool's chunks already queued: the memory is freed in the pool stream's
+ * order after them, and kept reserved for the next members. */
 int d3q19_pool_release(d3q19_pool* pool, int slot);
 /* Pre-emption: d3q19_pool_evict writes the member's checkpoint to buf
  * (d3q19_checkpoint_bytes of d3q19_pool_context(slot)) and releases the
