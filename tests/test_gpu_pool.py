@@ -161,3 +161,33 @@ def test_batched_stress_matches_per_member():
     free = [k for k in range(6) if k not in slots]
     assert all(code[k] == -1 and np.isnan(st[k]) for k in free)
     pool.close()
+
+
+def test_server_preemption_changes_no_result():
+    # A pool that holds two of the six solves at a time, served in arrival
+    # order and with pre-emption: evicted solves continue from their
+    # checkpoints, so every solve ends with the same steps and bit-identical
+    # stress and viscosity either way.
+    reqs = [sv.ShearRequest(rid=i, edge=(32 + 2 * (i % 3),) * 3, phi=0.1, model=sv.MODELS[i % 3], wall_speed=0.02,
+                            seed=20 + i, arrival=0.0) for i in range(6)]
+    need = 0
+    for r in reqs:
+        h = sv.host_state(r)
+        opt = d3.Options.from_buffer_copy(bytes(h.options))
+        opt.storage = 1
+        need = max(need, d3.context_bytes(h.cfg.ip, opt))
+    probe = d3.Pool(storage=1, max_slots=6)
+    base, _, _ = probe.usage()
+    probe.close()
+    out = {}
+    for pre in (None, 300):
+        pool = d3.Pool(storage=1, max_slots=6, hbm_budget=base + 2 * need + need // 2)
+        recs, _ = sv.Server(pool, check_every=100, rel_tol=1e-12, max_steps=1500, builders=0,
+                            preempt_after=pre).run(reqs)
+        assert pool.usage()[2] == 0
+        pool.close()
+        out[pre] = {r.rid: r for r in recs}
+    assert sum(r.preempted for r in out[300].values()) > 0
+    for i in range(6):
+        a, b = out[None][i], out[300][i]
+        assert a.steps == b.steps and a.stress == b.stress and a.eff_viscosity == b.eff_viscosity, i
