@@ -521,12 +521,28 @@ def run_batch(args):
             "speedup_vs_one_at_a_time_fp32": round(batched / alone, 2)}
 
 
+def warm_served_paths(storages, alone=True):
+    """Untimed: a short burst through a pool of each storage (and, with
+    alone, one solve on its own context), so that the timed runs do not pay
+    the first use of the kernels, graphs and allocators."""
+    import d3q19_b200 as d3
+    from d3q19_b200 import serving as sv
+
+    reqs = sv.make_requests(12, 0.0, 99, edges=(32, 64))
+    for storage in storages:
+        pool = d3.Pool(storage=storage, max_slots=64, hbm_budget=4 << 30)
+        sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=2000).run(reqs)
+        pool.close()
+    if alone:
+        sv.one_at_a_time(reqs[:2], storage=0, check_every=500, rel_tol=1e-4, max_steps=2000)
+
+
 def run_served(args):
     """cfg: Poisson arrivals (50/s, seeded) of shear-rheology solves, cubic
     edge in [32, 64], volume fraction in [0, 0.3], Newtonian / power law /
     Casson, each until the mean shear stress changes < 1e-4 relative over 500
-    steps (at most max_steps); FP16 pool with continuous batching against
-    one-at-a-time FP32."""
+    steps (at most max_steps); a pool with continuous batching (FP32 storage;
+    FP16 shifted storage reported beside it) against one-at-a-time FP32."""
     import numpy as np
     import torch
 
@@ -536,32 +552,41 @@ def run_served(args):
     torch.cuda.set_device(0)
     reqs = sv.make_requests(args.requests, 50.0, 2024, edges=(32, 64))
     max_steps = 40000
-    pool = d3.Pool(storage=1, max_slots=256, hbm_budget=100 << 30)
-    recs, wall = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=max_steps).run(reqs)
-    pool.close()
-    served = sv.summary(recs, wall)
+    warm_served_paths((0, 1))
+    runs = {}
+    for storage in (0, 1):
+        pool = d3.Pool(storage=storage, max_slots=256, hbm_budget=100 << 30)
+        runs[storage] = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=max_steps).run(reqs)
+        pool.close()
+    served, served16 = sv.summary(*runs[0]), sv.summary(*runs[1])
     base, bwall = sv.one_at_a_time(reqs, storage=0, check_every=500, rel_tol=1e-4, max_steps=max_steps)
     alone = sv.summary(base, bwall)
     by = {r.rid: r for r in base}
-    visc_err = [abs(r.eff_viscosity - by[r.rid].eff_viscosity) / max(abs(by[r.rid].eff_viscosity), 1e-30)
-                for r in recs if not (r.failed or by[r.rid].failed)]
+
+    def visc_diff(recs):
+        d = [abs(r.eff_viscosity - by[r.rid].eff_viscosity) / max(abs(by[r.rid].eff_viscosity), 1e-30)
+             for r in recs if not (r.failed or by[r.rid].failed)]
+        return {"max": float(np.max(d)), "median": float(np.median(d))}
+
+    recs = runs[0][0]
     return {"metric": "solves/s (served sweep)", "value": round(served["solves_per_s"], 3), "unit": "solves/s",
-            "n_gpus": 1, "higher_is_better": True, "dtype": "f32 arithmetic, f16 shifted storage",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
             "data": "synthetic (seeded Poisson arrivals)", "impl": "ours",
             "config": {"workload": "served-sweep", "requests": len(reqs), "arrival_rate_per_s": 50.0,
                        "edges": [32, 64], "phi": [0.0, 0.3], "models": list(sv.MODELS), "stop": "1e-4 over 500 steps",
-                       "max_steps": max_steps},
-            "served": served, "one_at_a_time_fp32": alone,
+                       "max_steps": max_steps, "pool_storage": "fp32"},
+            "served": served, "served_fp16_pool": served16, "one_at_a_time_fp32": alone,
             "speedup_solves_per_s": round(served["solves_per_s"] / alone["solves_per_s"], 2),
+            "speedup_fp16_pool": round(served16["solves_per_s"] / alone["solves_per_s"], 2),
             "per_request": [[r.rid, r.steps, by[r.rid].steps, round(r.latency, 3), round(by[r.rid].latency, 3)]
                             for r in sorted(recs, key=lambda r: r.rid)],
-            "eff_viscosity_rel_diff_fp16_pool_vs_fp32_alone": {"max": float(np.max(visc_err)),
-                                                               "median": float(np.median(visc_err))}}
+            "eff_viscosity_rel_diff_pool_vs_alone": visc_diff(recs),
+            "eff_viscosity_rel_diff_fp16_pool_vs_alone": visc_diff(runs[1][0])}
 
 
 def run_served_preempt(args):
-    """cfg: the served sweep's Poisson arrivals (50/s, seeded) on an FP16 pool
-    whose HBM budget holds a few members at a time, served twice: admission
+    """cfg: the served sweep's Poisson arrivals (50/s, seeded) on an FP32 pool
+    whose HBM budget (256 MB) holds a few members at a time, served twice: admission
     in arrival order only, and with pre-emption (a request that does not fit
     evicts the member with the most steps since its admission, once that is
     at least 2000; the evicted member's checkpoint waits in host memory and
@@ -576,10 +601,11 @@ def run_served_preempt(args):
     torch.cuda.set_device(0)
     reqs = sv.make_requests(args.requests, 50.0, 2025, edges=(32, 64))
     max_steps = 40000
-    budget = 160 << 20
+    budget = 256 << 20
+    warm_served_paths((0,), alone=False)
     out = {}
     for label, pre in (("arrival_order", None), ("preempt_2000", 2000)):
-        pool = d3.Pool(storage=1, max_slots=64, hbm_budget=budget)
+        pool = d3.Pool(storage=0, max_slots=64, hbm_budget=budget)
         cost = {"evict_s": 0.0, "readmit_s": 0.0, "bytes": 0, "n": 0}
         ev, re = pool.evict, pool.readmit
 
@@ -614,7 +640,7 @@ def run_served_preempt(args):
         del v["latency_by_rid"]
     return {"metric": "solves/s (served sweep, HBM-limited pool)", "value": round(b["solves_per_s"], 3),
             "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
-            "dtype": "f32 arithmetic, f16 shifted storage", "data": "synthetic (seeded Poisson arrivals)",
+            "dtype": "f32", "data": "synthetic (seeded Poisson arrivals)",
             "impl": "ours",
             "config": {"workload": "served-preempt", "requests": len(reqs), "arrival_rate_per_s": 50.0,
                        "edges": [32, 64], "phi": [0.0, 0.3], "models": list(sv.MODELS), "hbm_budget_mb": budget >> 20,
