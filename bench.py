@@ -13,6 +13,14 @@ Metric: MLUPS = interior nodes x steps / s / 1e6, summed over GPUs (each GPU
 runs an independent replica: weak scaling, no collective on the data path).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Other modes (--workload, one GPU, one JSON line each): powerlaw-128-fluid and
+couette-sphere-64 (the same line for the fluid alone and the 64^3 single
+sphere); batch-64 (64 uneven boxes in one lattice pool against each alone);
+served-sweep (Poisson arrivals of shear-rheology solves through the pool's
+serving loop against one at a time); served-preempt (the same on a pool
+with a small HBM budget, with and without pre-emption); casson-precision
+(FP32 / FP16 / BF16 storage against the FP64 build).
 """
 import argparse
 import json
