@@ -1330,8 +1330,13 @@ struct d3q19_pool {
   size_t stats_cap = 0;
   std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  // (steps, fblocks, pblocks, cblocks)
   long long steps = 0;
+  // Every d3q19_pool_* call holds it: the pool may be driven from several
+  // host threads (its members are not stepped outside these calls).
+  std::mutex mu;
   char msg[512] = {0};
 };
+
+#define POOL_LOCK(p) std::lock_guard<std::mutex> pool_lock_((p)->mu)
 
 static int pfail(d3q19_pool* p, int code, const char* fmt, ...) {
   char* buf = p ? p->msg : g_create_error;
@@ -1441,6 +1446,7 @@ extern "C" int d3q19_pool_admit(d3q19_pool* p, const int_param_struct* ip, const
                                 const float* spherePoints, const int* zoneNeighDat, const int* parsZone,
                                 const int* zoneMembers, const int* numParInZone, int* slot_out) {
   if (!p || !ip || !fp || !f || !u || !slot_out) return D3Q19_EINVAL;
+  POOL_LOCK(p);
   d3q19_options o;
   int s = -1;
   size_t bytes = 0;
@@ -1558,6 +1564,7 @@ static int pool_enqueue(d3q19_pool* p, int nsteps) {
 
 extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
   if (!p) return D3Q19_EINVAL;
+  POOL_LOCK(p);
   if (nsteps <= 0 || nsteps % p->period != 0)
     return pfail(p, D3Q19_EINVAL, "steps must be a positive multiple of %d", p->period);
   cudaSetDevice(p->dev);
@@ -1601,6 +1608,7 @@ extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
 extern "C" int d3q19_pool_mean_stress(d3q19_pool* p, double* stress_xz, double* shear_rate, double* eff_viscosity,
                                       int* status) {
   if (!p || !stress_xz || !status) return D3Q19_EINVAL;
+  POOL_LOCK(p);
   cudaSetDevice(p->dev);
   // Layout: per member, 5*Nz plane sums then its error word.
   std::vector<size_t> off(p->max_slots, 0);
@@ -1661,17 +1669,21 @@ extern "C" int d3q19_pool_mean_stress(d3q19_pool* p, double* stress_xz, double* 
 }
 
 extern "C" d3q19_ctx* d3q19_pool_context(d3q19_pool* p, int slot) {
-  if (!p || slot < 0 || slot >= p->max_slots) return nullptr;
-  return p->slot[slot];
+  if (!p || slot < 0) return nullptr;
+  POOL_LOCK(p);
+  return slot < p->max_slots ? p->slot[slot] : nullptr;
 }
 
 extern "C" long long d3q19_pool_slot_steps(d3q19_pool* p, int slot) {
-  if (!p || slot < 0 || slot >= p->max_slots || !p->slot[slot]) return -1;
+  if (!p || slot < 0) return -1;
+  POOL_LOCK(p);
+  if (slot >= p->max_slots || !p->slot[slot]) return -1;
   return p->slot_steps[slot];
 }
 
-extern "C" int d3q19_pool_release(d3q19_pool* p, int slot) {
-  if (!p || slot < 0 || slot >= p->max_slots || !p->slot[slot]) return D3Q19_EINVAL;
+// Release with the pool's lock held.
+static int release_slot(d3q19_pool* p, int slot) {
+  if (slot < 0 || slot >= p->max_slots || !p->slot[slot]) return D3Q19_EINVAL;
   cudaSetDevice(p->dev);
   // No wait for the chunks in flight: the member's memory is freed in the
   // pool stream's order, after them (its own streams are drained by destroy).
@@ -1686,18 +1698,27 @@ extern "C" int d3q19_pool_release(d3q19_pool* p, int slot) {
   return 0;
 }
 
+extern "C" int d3q19_pool_release(d3q19_pool* p, int slot) {
+  if (!p) return D3Q19_EINVAL;
+  POOL_LOCK(p);
+  return release_slot(p, slot);
+}
+
 extern "C" int d3q19_pool_evict(d3q19_pool* p, int slot, void* buf, size_t bytes) {
-  if (!p || slot < 0 || slot >= p->max_slots || !p->slot[slot]) return D3Q19_EINVAL;
+  if (!p) return D3Q19_EINVAL;
+  POOL_LOCK(p);
+  if (slot < 0 || slot >= p->max_slots || !p->slot[slot]) return D3Q19_EINVAL;
   cudaSetDevice(p->dev);
   POOL_TRY(p, cudaStreamSynchronize(p->stream));
   d3q19_ctx* c = p->slot[slot];
   if (int rc = d3q19_checkpoint(c, buf, bytes)) return pfail(p, rc, "%s", d3q19_last_error(c));
-  return d3q19_pool_release(p, slot);
+  return release_slot(p, slot);
 }
 
 extern "C" int d3q19_pool_readmit(d3q19_pool* p, const int_param_struct* ip, const flp_param_struct* fp,
                                   const d3q19_options* opt, const void* buf, size_t bytes, int* slot_out) {
   if (!p || !ip || !fp || !buf || !slot_out) return D3Q19_EINVAL;
+  POOL_LOCK(p);
   if (bytes < sizeof(CkptHeader)) return pfail(p, D3Q19_EINVAL, "not a checkpoint");
   CkptHeader h;
   memcpy(&h, buf, sizeof(h));
@@ -1728,6 +1749,7 @@ extern "C" int d3q19_pool_readmit(d3q19_pool* p, const int_param_struct* ip, con
 
 extern "C" int d3q19_pool_usage(d3q19_pool* p, size_t* used, size_t* budget, int* members) {
   if (!p) return D3Q19_EINVAL;
+  POOL_LOCK(p);
   int n = 0;
   for (auto* c : p->slot) n += c != nullptr;
   if (used) *used = p->used;
@@ -1738,6 +1760,7 @@ extern "C" int d3q19_pool_usage(d3q19_pool* p, size_t* used, size_t* budget, int
 
 extern "C" int d3q19_pool_set_grid(d3q19_pool* p, int fluid_blocks, int particle_blocks, int contact_blocks) {
   if (!p || fluid_blocks <= 0 || particle_blocks <= 0 || contact_blocks <= 0) return D3Q19_EINVAL;
+  POOL_LOCK(p);
   p->fblocks = fluid_blocks;
   p->pblocks = particle_blocks;
   p->cblocks = contact_blocks;
@@ -1746,6 +1769,7 @@ extern "C" int d3q19_pool_set_grid(d3q19_pool* p, int fluid_blocks, int particle
 
 extern "C" int d3q19_pool_get_grid(d3q19_pool* p, int* fluid_blocks, int* particle_blocks, int* contact_blocks) {
   if (!p) return D3Q19_EINVAL;
+  POOL_LOCK(p);
   if (fluid_blocks) *fluid_blocks = p->fblocks;
   if (particle_blocks) *particle_blocks = p->pblocks;
   if (contact_blocks) *contact_blocks = p->cblocks;
@@ -1754,6 +1778,7 @@ extern "C" int d3q19_pool_get_grid(d3q19_pool* p, int* fluid_blocks, int* partic
 
 extern "C" int d3q19_pool_synchronize(d3q19_pool* p) {
   if (!p) return D3Q19_EINVAL;
+  POOL_LOCK(p);
   cudaSetDevice(p->dev);
   POOL_TRY(p, cudaStreamSynchronize(p->stream));
   for (int s = 0; s < p->max_slots; s++)
@@ -1769,6 +1794,8 @@ extern "C" const char* d3q19_pool_last_error(d3q19_pool* p) { return p ? p->msg 
 
 extern "C" int d3q19_pool_destroy(d3q19_pool* p) {
   if (!p) return D3Q19_EINVAL;
+  // Waits for a call in progress on another thread; none may start after it.
+  { POOL_LOCK(p); }
   cudaSetDevice(p->dev);
   if (p->stream) cudaStreamSynchronize(p->stream);
   pool_drop_graphs(p);

@@ -321,6 +321,11 @@ int d3q19_destroy(d3q19_ctx* ctx);
  * members.
  * ------------------------------------------------------------------------- */
 typedef struct d3q19_pool d3q19_pool;
+/* Threads: every d3q19_pool_* call holds the pool's lock, so several host
+ * threads may admit, release, read and advance the same pool (for example one
+ * thread admitting arrivals while another drives the chunks).  A member's
+ * context (d3q19_pool_context) is for read-backs between calls; it is not
+ * stepped on its own.  d3q19_pool_last_error is per pool, not per thread. */
 
 /* Device memory d3q19_create allocates for these parameters (read-back
  * scratch, allocated on first use, not included). */

@@ -191,3 +191,47 @@ def test_server_preemption_changes_no_result():
     for i in range(6):
         a, b = out[None][i], out[300][i]
         assert a.steps == b.steps and a.stress == b.stress and a.eff_viscosity == b.eff_viscosity, i
+
+
+def test_pool_driven_from_several_threads():
+    # Every pool call holds the pool's lock: members admitted from four
+    # threads at once, and a member admitted while another thread advances
+    # the pool, end bit for bit like the same solves alone.
+    import threading
+
+    pool = d3.Pool(storage=1, max_slots=8)
+    states = [sv.host_state(r) for r in REQS]
+    slots = [None] * 4
+    errs = []
+
+    def admit(k):
+        try:
+            slots[k] = pool.admit(states[k])
+        except Exception as e:  # noqa: BLE001 - reported by the assert below
+            errs.append(e)
+
+    th = [threading.Thread(target=admit, args=(k,)) for k in range(3)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs and None not in slots[:3]
+
+    def drive():
+        try:
+            for _ in range(5):
+                pool.advance(20)
+        except Exception as e:  # noqa: BLE001
+            errs.append(e)
+
+    t = threading.Thread(target=drive)
+    t.start()
+    admit(3)  # while the chunks run
+    t.join()
+    pool.advance(20)
+    assert not errs and slots[3] is not None
+    got = {k: (state(pool, slots[k]), pool.steps(slots[k]) - pool.period) for k in range(4)}
+    pool.close()
+    assert got[0][1] == 120
+    for k in range(4):
+        bits_equal(got[k][0], alone(REQS[k], 1, [got[k][1]]))
