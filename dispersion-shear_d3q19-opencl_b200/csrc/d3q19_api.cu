@@ -1776,6 +1776,16 @@ extern "C" int d3q19_pool_get_grid(d3q19_pool* p, int* fluid_blocks, int* partic
   return 0;
 }
 
+extern "C" int d3q19_pool_poll(d3q19_pool* p) {
+  if (!p) return D3Q19_EINVAL;
+  POOL_LOCK(p);
+  cudaSetDevice(p->dev);
+  const cudaError_t e = cudaEventQuery(p->ev_done);
+  if (e == cudaSuccess) return 1;
+  if (e == cudaErrorNotReady) return 0;
+  return pfail(p, D3Q19_ECUDA, "cudaEventQuery: %s", cudaGetErrorString(e));
+}
+
 extern "C" int d3q19_pool_synchronize(d3q19_pool* p) {
   if (!p) return D3Q19_EINVAL;
   POOL_LOCK(p);

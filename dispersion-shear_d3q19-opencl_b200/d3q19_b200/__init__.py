@@ -136,6 +136,7 @@ def cuda_lib():
         lib.d3q19_pool_set_grid.argtypes = [P, C.c_int, C.c_int, C.c_int]
         lib.d3q19_pool_get_grid.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         lib.d3q19_pool_synchronize.argtypes = [P]
+        lib.d3q19_pool_poll.argtypes = [P]
         lib.d3q19_pool_stream.restype = P
         lib.d3q19_pool_stream.argtypes = [P]
         lib.d3q19_pool_last_error.restype = C.c_char_p
@@ -593,6 +594,13 @@ class Pool:
 
     def synchronize(self):
         self._check(self.lib.d3q19_pool_synchronize(self.h), "pool_synchronize")
+
+    def poll(self) -> bool:
+        """Whether the last advance has finished on the device (no wait)."""
+        rc = self.lib.d3q19_pool_poll(self.h)
+        if rc < 0:
+            self._check(rc, "pool_poll")
+        return rc == 1
 
     @property
     def stream_ptr(self) -> int:

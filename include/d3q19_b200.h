@@ -379,6 +379,10 @@ int d3q19_pool_usage(d3q19_pool* pool, size_t* used, size_t* budget, int* member
  * passes; the autotuner sets them.  Results do not depend on them. */
 int d3q19_pool_set_grid(d3q19_pool* pool, int fluid_blocks, int particle_blocks, int contact_blocks);
 int d3q19_pool_get_grid(d3q19_pool* pool, int* fluid_blocks, int* particle_blocks, int* contact_blocks);
+/* Without waiting: 1 when the work of the last d3q19_pool_advance has
+ * finished on the device (or none was queued), 0 while it runs, negative on
+ * a CUDA error.  For callers that run their own event loop. */
+int d3q19_pool_poll(d3q19_pool* pool);
 /* Waits for the pool's work and reports the members' device errors. */
 int d3q19_pool_synchronize(d3q19_pool* pool);
 /* The pool's CUDA stream (cudaStream_t). */

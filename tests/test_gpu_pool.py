@@ -235,3 +235,19 @@ def test_pool_driven_from_several_threads():
     assert got[0][1] == 120
     for k in range(4):
         bits_equal(got[k][0], alone(REQS[k], 1, [got[k][1]]))
+
+
+def test_poll_reports_the_chunk_without_waiting():
+    import time
+
+    pool = d3.Pool(storage=1, max_slots=2)
+    assert pool.poll()  # nothing queued yet
+    pool.admit(sv.host_state(REQS[1]))
+    pool.advance(2000)
+    t0 = time.perf_counter()
+    while not pool.poll():
+        assert time.perf_counter() - t0 < 60.0
+        time.sleep(0.001)
+    pool.synchronize()
+    assert pool.poll()
+    pool.close()
