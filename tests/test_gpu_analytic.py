@@ -165,5 +165,82 @@ def test_poiseuille_matches_the_law(case, arith):
     assert drift < max(tol / 10, 1e-6) and err < tol, (drift, err, float(np.max(u)), float(np.max(want)))
 
 
+
+
+def fixed_sphere(L, g, d=8.0, steps=40000, arithmetic=0):
+    """A sphere held fixed at the centre of a fully periodic L^3 lattice,
+    fluid driven by the body force g along x.  Returns the x force of the
+    fluid on the sphere (the sum of its marker forces), its change over the
+    last 5000 steps, and the mean fluid velocity (superficial velocity)."""
+    S = L - 2
+    kw = dict(iterations=10 ** 6, total_lattice_size=(L, L, L), boundary_conditions_xyz=(0, 0, 0),
+              newtonian_tau=1.0, viscosity_model=1, use_constant_viscosity=1, constant_body_force=(g, 0.0, 0.0),
+              initial_f="constant", initial_vel=(0.0, 0.0, 0.0), domain_decomposition=(1, 1, 1), num_particles=1,
+              particle_diameter=d, initial_particle_distribution=3, initial_particle_buffer=S / 2.0,
+              fixed_particles=1, rebuild_neigh_list_freq=10, video_freq=10 ** 9, shear_stress_freq=10 ** 9,
+              console_print_freq=10 ** 9)
+    sim = d3.Simulation.from_host_state(d3.HostState(d3.parse_config(d3.keywords_text(kw))), arithmetic=arithmetic)
+
+    def force():
+        pff = sim.read_parfluidforce().reshape(2, sim.np, sim.nfa, 4).astype(np.float64)
+        return float(pff[0, 0, :, 0].sum())
+
+    # The direct-forcing feedback leaves a small step-to-step alternation in
+    # the marker force: the balance is checked on the mean of two steps.
+    sim.run(1, steps - 5000)
+    f0 = force()
+    sim.run(steps - 4999, 5000)
+    f1 = force()
+    sim.run(steps + 1, 1)
+    f1 = 0.5 * (f1 + force())
+    u = sim.read_u()[:sim.nc].reshape(L, L, L)[1:L - 1, 1:L - 1, 1:L - 1].astype(np.float64)
+    sim.close()
+    return f1, abs(f1 - f0) / abs(f1), float(u.mean()), S ** 3
+
+
+def hasimoto_radius(F, U, L_int, nu=1.0 / 6.0):
+    """Radius a of a sphere in a simple cubic array of period L_int whose
+    Stokes drag 6 pi mu a U / K(c) (Hasimoto's series, c the volume
+    fraction) equals F."""
+    def drag(a):
+        c = 4.0 / 3.0 * np.pi * a ** 3 / L_int ** 3
+        K = 1.0 - 1.7601 * c ** (1.0 / 3.0) + c - 1.5593 * c ** 2
+        return 6.0 * np.pi * nu * a * U / K
+
+    lo, hi = 0.5, 0.3 * L_int
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if drag(mid) < F else (lo, mid)
+    return 0.5 * (lo + hi)
+
+
+@pytest.mark.parametrize("arith", [0, 2], ids=["fp32", "fp64-build"])
+def test_fixed_sphere_drag(arith):
+    # Exact: at steady state nothing else holds the fluid back, so the
+    # marker forces on the sphere add up to the body force on all nodes.
+    # The FP64 build holds this to 1e-4 (the remaining transient).  In FP32
+    # the body force of 1e-6 per node is only ~45 ulp of a population near
+    # 1/18, and its rounding is correlated between nodes: the momentum it
+    # adds is off by up to ~0.7 % (0.69 % in a box without the sphere), so
+    # FP32 is held to 1 %.
+    # Functional form (FP64): the hydrodynamic radius that Hasimoto's
+    # periodic-array drag implies is the same in two box sizes, and the drag
+    # is linear in the driving force (Stokes regime, Re ~ 0.1).
+    g = 1e-6
+    out = {}
+    for L in (34, 42):
+        F, drift, U, n = fixed_sphere(L, g, steps=60000, arithmetic=arith)
+        out[L] = (F, drift, U, n, hasimoto_radius(F, U, L - 2))
+    MEASURED[f"sphere/{arith}"] = {L: (v[0] / (g * v[3]) - 1.0, v[1], v[4]) for L, v in out.items()}
+    bal = 1e-4 if arith else 1e-2
+    for L, (F, drift, U, n, a) in out.items():
+        assert drift < 1e-3 and abs(F / (g * n) - 1.0) < bal, (L, F, g * n, drift)
+    if arith:
+        F2, _, U2, _ = fixed_sphere(34, 2 * g, steps=60000, arithmetic=arith)
+        MEASURED["sphere_linearity"] = (F2 / out[34][0] - 2.0, U2 / out[34][2] - 2.0)
+        assert abs(out[34][4] / out[42][4] - 1.0) < 0.02 and 2.0 < out[34][4] < 5.0, (out[34][4], out[42][4])
+        assert abs(F2 / out[34][0] - 2.0) < 1e-4 and abs(U2 / out[34][2] - 2.0) < 3e-2
+
+
 def test_zz_report_measured_errors():
-    print("analytic profile errors:", {k: float(f"{v:.3g}") for k, v in MEASURED.items()})
+    print("analytic errors:", MEASURED)
