@@ -251,3 +251,46 @@ def test_poll_reports_the_chunk_without_waiting():
     pool.synchronize()
     assert pool.poll()
     pool.close()
+
+
+def test_non_finite_member_is_reported_and_isolated():
+    # A NaN planted (from the host) in one member's populations: the device
+    # error word of that member reports it (ENUMERIC) while the other member
+    # runs on bit for bit as alone, and the GPU stays usable.
+    pool = d3.Pool(storage=0, max_slots=4)
+    sa = pool.admit(sv.host_state(REQS[0]))
+    sb = pool.admit(sv.host_state(REQS[2]))
+    m = pool.member(sb)
+    f = m.read_f()
+    N = m.ip.LatticeSize
+    centre = N[0] // 2 + N[0] * (N[1] // 2 + N[1] * (N[2] // 2))  # an interior node
+    f[5 * m.nc + centre] = np.nan
+    m.write_lattice(f, m.read_u(), m.read_tau())
+    pool.advance(20)
+    st, _, _, code = pool.mean_stress_all(4)
+    assert d3.STATUS[int(code[sb])] == "ENUMERIC" and code[sa] == 0 and np.isfinite(st[sa])
+    pool.release(sb)
+    pool.advance(20)
+    got = state(pool, sa)
+    pool.close()
+    bits_equal(got, alone(REQS[0], 0, [40]))
+
+
+def test_non_finite_state_is_reported_by_a_context():
+    hs = sv.host_state(REQS[2])
+    sim = d3.Simulation.from_host_state(hs)
+    f = np.array(hs.f, np.float32, copy=True).reshape(-1)
+    N = sim.ip.LatticeSize
+    f[3 * sim.nc + N[0] // 2 + N[0] * (N[1] // 2 + N[1] * (N[2] // 2))] = np.inf  # an interior node
+    sim.write_lattice(f, hs.u, hs.tau)
+    sim.run(1, 4)
+    with pytest.raises(d3.D3Q19Error, match="ENUMERIC"):
+        sim.synchronize()
+    with pytest.raises(d3.D3Q19Error, match="ENUMERIC"):  # sticky: reported by every later call
+        sim.read_u()
+    sim.close()
+    ok = d3.Simulation.from_host_state(hs)
+    ok.run(1, 4)
+    ok.synchronize()
+    assert np.isfinite(ok.read_u()).all()
+    ok.close()
