@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import threading
 import time
 from concurrent.futures import Future, ThreadPoolExecutor
 
@@ -117,6 +118,7 @@ class SolveRecord:
     converged: bool
     failed: bool = False  # the solve stopped on a device error (non-finite state)
     preempted: int = 0    # times the solve was evicted and re-admitted
+    cancelled: bool = False  # stopped by Server.cancel
 
     @property
     def latency(self) -> float:
@@ -146,6 +148,7 @@ def summary(records: list, wall: float) -> dict:
             "converged": int(sum(r.converged for r in records)),
             "failed": int(sum(r.failed for r in records)),
             "preempted": int(sum(r.preempted for r in records)),
+            "cancelled": int(sum(r.cancelled for r in records)),
             "steps": int(sum(r.steps for r in records))}
 
 
@@ -169,7 +172,11 @@ class Server:
     of the queue does not fit, the member with the most steps since its
     (re)admission is evicted if that count is at least preempt_after, and
     again until the request fits or no member qualifies.  An evicted member
-    is re-admitted before any request that arrived after its eviction."""
+    is re-admitted before any request that arrived after its eviction.
+
+    cancel(rid), from any thread, stops a request at the next chunk
+    boundary: a queued one is never admitted, a running one is released, a
+    parked one drops its checkpoint; its record has cancelled = True."""
 
     def __init__(self, pool: Pool, check_every: int = 500, rel_tol: float = 1e-4, max_steps: int = 20000,
                  clock=time.perf_counter, sleep=time.sleep, builders: int = 4, preempt_after: int | None = None):
@@ -185,6 +192,17 @@ class Server:
         self.sleep = sleep
         self.builders = builders
         self.preempt_after = preempt_after
+        self._lock = threading.Lock()
+        self._cancel = set()
+
+    def cancel(self, rid: int):
+        """Asks to stop request rid (takes effect at the next chunk boundary)."""
+        with self._lock:
+            self._cancel.add(rid)
+
+    def _cancelled(self):
+        with self._lock:
+            return set(self._cancel)
 
     def _stresses(self, active):
         """{slot: (stress, viscosity) or None for a failed member}."""
@@ -261,6 +279,7 @@ class Server:
             # at the first one that does not fit.
             nonlocal qi
             prepare()
+            cancel_requested()
             while True:
                 if parked and parked[0][0] <= qi:
                     _, m, ck = parked[0]
@@ -287,8 +306,44 @@ class Server:
                 joining[slot] = _Member(req, self.clock() - t0, Convergence(self.rel_tol), self.pool.steps(slot))
                 qi += 1
 
+        def cancel_requested():
+            # Queued, parked and running requests asked to stop.
+            nonlocal nb
+            gone = self._cancelled()
+            if not gone:
+                return
+            now = self.clock() - t0
+            for members in (active, joining):
+                for slot in [s for s, m in members.items() if m.req.rid in gone]:
+                    m = members.pop(slot)
+                    done.append(SolveRecord(m.req.rid, m.req.arrival, m.start, now, self.pool.steps(slot),
+                                            float("nan"), float("nan"), False, False, m.preempted, True))
+                    self.pool.release(slot)
+            for entry in [e for e in parked if e[1].req.rid in gone]:
+                parked.remove(entry)
+                m = entry[1]
+                done.append(SolveRecord(m.req.rid, m.req.arrival, m.start, now, 0, float("nan"), float("nan"), False,
+                                        False, m.preempted, True))
+            # Queued requests leave the queue; the ones behind them move up.
+            dropped = [k for k in range(qi, len(queue)) if queue[k].rid in gone]
+            if dropped:
+                for k in dropped:
+                    req = queue[k]
+                    built.pop(req.rid, None)
+                    done.append(SolveRecord(req.rid, req.arrival, now, now, 0, float("nan"), float("nan"), False,
+                                            False, 0, True))
+                nb -= sum(1 for k in dropped if k < nb)
+                for j, (mark, m, ck) in enumerate(parked):
+                    parked[j] = (mark - sum(1 for k in dropped if k < mark), m, ck)
+                queue[:] = [r for k, r in enumerate(queue) if k < qi or r.rid not in gone]
+            with self._lock:
+                self._cancel -= gone
+
         try:
             while qi < len(queue) or active or joining or parked:
+                cancel_requested()
+                if not (qi < len(queue) or active or joining or parked):
+                    break
                 # Between chunks the GPU waits for the host, so requests are
                 # admitted here only into an empty pool; otherwise they are
                 # admitted while the next chunk runs.  Evictions need the

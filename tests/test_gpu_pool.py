@@ -294,3 +294,27 @@ def test_non_finite_state_is_reported_by_a_context():
     ok.synchronize()
     assert np.isfinite(ok.read_u()).all()
     ok.close()
+
+
+def test_server_cancels_queued_and_running_requests():
+    reqs = [sv.ShearRequest(rid=i, edge=(32, 32, 32), phi=0.1, model=sv.MODELS[i % 3], wall_speed=0.02,
+                            seed=30 + i, arrival=0.0) for i in range(4)]
+    pool = d3.Pool(storage=0, max_slots=8)
+    srv = sv.Server(pool, check_every=100, rel_tol=1e-12, max_steps=1000, builders=0)
+    srv.cancel(3)
+    advance, chunks = pool.advance, []
+
+    def advance_then_cancel(n):  # as another thread would, while chunk 2 runs
+        advance(n)
+        chunks.append(n)
+        if len(chunks) == 2:
+            srv.cancel(1)
+
+    pool.advance = advance_then_cancel
+    recs, _ = srv.run(reqs)
+    by = {r.rid: r for r in recs}
+    assert by[3].cancelled and by[3].steps == 0
+    assert by[1].cancelled and by[1].steps < 1000
+    assert not by[0].cancelled and by[0].steps >= 1000 and np.isfinite(by[0].stress)
+    assert pool.usage()[2] == 0
+    pool.close()

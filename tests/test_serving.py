@@ -241,3 +241,45 @@ def test_preempted_member_is_not_starved():
 def test_preempt_after_must_be_positive():
     with pytest.raises(ValueError):
         sv.Server(FakePool(10), check_every=500, preempt_after=0)
+
+
+def test_cancel_queued_running_and_parked():
+    reqs = [sv.ShearRequest(rid=i, edge=(32, 32, 32), phi=0.0, model="newtonian", wall_speed=0.02, seed=1,
+                            arrival=1e-3 * i) for i in range(5)]
+    clock = {"t": 0.0}
+
+    def now():
+        clock["t"] += 1e-4
+        return clock["t"]
+
+    class HookPool(FakePool):
+        # Calls the hook after every advance, as another thread would.
+        hook = None
+
+        def advance(self, n):
+            super().advance(n)
+            if self.hook:
+                self.hook(self)
+
+    pool = HookPool(budget=20)
+    srv = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=60000, clock=now,
+                    sleep=lambda dt: clock.__setitem__("t", clock["t"] + dt), builders=0, preempt_after=1000)
+    build = lambda r: {"bytes": 10, "rid": r.rid, "target": 1.0, "tconst": 3000.0 if r.rid in (0, 1) else 300.0}
+    srv.cancel(4)  # queued: never admitted
+
+    def hook(p):
+        members = {p.rid[s]: s for s in p.size}
+        if 0 in members and p.steps_done[members[0]] >= 2000:
+            srv.cancel(0)  # running
+        if 1 in p.evicted and 1 not in members and 1 not in p.readmitted:
+            srv.cancel(1)  # parked after its eviction
+
+    pool.hook = hook
+    recs, _ = srv.run(reqs, build=build)
+    by = {r.rid: r for r in recs}
+    assert sorted(by) == [0, 1, 2, 3, 4]
+    assert by[4].cancelled and by[4].steps == 0 and 4 not in pool.admitted
+    assert by[0].cancelled and 2000 <= by[0].steps < 60000
+    assert all(by[k].converged and not by[k].cancelled for k in (2, 3))
+    assert pool.used == 0 and sv.summary(recs, 1.0)["cancelled"] == sum(r.cancelled for r in recs)
+    assert 1 in pool.evicted and by[1].cancelled and 1 not in pool.readmitted
