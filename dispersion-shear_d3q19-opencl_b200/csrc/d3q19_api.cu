@@ -4,6 +4,7 @@
 #include "d3q19_internal.h"
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdarg>
@@ -20,6 +21,16 @@ static_assert(sizeof(int_param_struct) == 332, "int_param_struct must match stru
 static_assert(sizeof(flp_param_struct) == 176, "flp_param_struct must match struct_header_device.h");
 
 using namespace d3q19;
+
+// NVTX range over an entry point: named spans on the host timeline of a
+// profiler such as Nsight Systems; no cost when no tool is attached.
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
+#define TRACE(name) TraceRange trace_range_(name)
 
 struct d3q19_ctx {
   int_param_struct ip;
@@ -205,6 +216,7 @@ static int create_ctx(const int_param_struct* ip, const flp_param_struct* fp, co
 
 extern "C" int d3q19_create(const int_param_struct* ip, const flp_param_struct* fp, const d3q19_options* opt,
                             d3q19_ctx** out) {
+  TRACE("d3q19_create");
   return create_ctx(ip, fp, opt, nullptr, out);
 }
 
@@ -725,6 +737,7 @@ static int join_side(d3q19_ctx* c) {
 }
 
 extern "C" int d3q19_step(d3q19_ctx* c, int t) {
+  TRACE("d3q19_step");
   int rc = check_ready(c);
   if (rc) return rc;
   if (c->kstage != 0) return fail(c, D3Q19_ESTATE, "step %d was left between passes", c->kt);
@@ -736,6 +749,7 @@ extern "C" int d3q19_step(d3q19_ctx* c, int t) {
 static int gcd_i(int a, int b) { return b ? gcd_i(b, a % b) : a; }
 
 extern "C" int d3q19_run(d3q19_ctx* c, int t0, int nsteps) {
+  TRACE("d3q19_run");
   int rc = check_ready(c);
   if (rc) return rc;
   if (c->kstage != 0) return fail(c, D3Q19_ESTATE, "step %d was left between passes", c->kt);
@@ -918,6 +932,7 @@ extern "C" int d3q19_read_zones(d3q19_ctx* c, int* parsZone, int* zoneMembers, i
 
 // Per-plane FP64 sums (plane_stats_kernel) of the last step, read back.
 extern "C" int d3q19_plane_stats(d3q19_ctx* c, double* out) {
+  TRACE("d3q19_plane_stats");
   if (!c || !out) return D3Q19_EINVAL;
   if (c->f_state == 0) return fail(c, D3Q19_ESTATE, "lattice not written");
   cudaSetDevice(c->dev);
@@ -961,6 +976,7 @@ extern "C" int d3q19_shear_profile(d3q19_ctx* c, double* u_mean, double* wall_ra
 }
 
 extern "C" int d3q19_mean_stress(d3q19_ctx* c, double* stress_xz, double* shear_rate, double* eff_viscosity) {
+  TRACE("d3q19_mean_stress");
   if (!c) return D3Q19_EINVAL;
   const int Nz = c->g.Nz;
   std::vector<double> ps(5 * (size_t)Nz);
@@ -1192,6 +1208,7 @@ extern "C" int d3q19_checkpoint_bytes(d3q19_ctx* c, size_t* bytes) {
 }
 
 extern "C" int d3q19_checkpoint(d3q19_ctx* c, void* buf, size_t bytes) {
+  TRACE("d3q19_checkpoint");
   if (!c || !buf) return D3Q19_EINVAL;
   if (c->f_state == 0) return fail(c, D3Q19_ESTATE, "lattice not written");
   if (c->kstage != 0) return fail(c, D3Q19_ESTATE, "step %d was left between passes", c->kt);
@@ -1230,6 +1247,7 @@ extern "C" int d3q19_checkpoint(d3q19_ctx* c, void* buf, size_t bytes) {
 }
 
 extern "C" int d3q19_restore(d3q19_ctx* c, const void* buf, size_t bytes) {
+  TRACE("d3q19_restore");
   if (!c || !buf || bytes < sizeof(CkptHeader)) return D3Q19_EINVAL;
   CkptHeader h;
   memcpy(&h, buf, sizeof(h));
@@ -1445,6 +1463,7 @@ extern "C" int d3q19_pool_admit(d3q19_pool* p, const int_param_struct* ip, const
                                 const float* parKin, const float* parForce, const float* parFluidForce,
                                 const float* spherePoints, const int* zoneNeighDat, const int* parsZone,
                                 const int* zoneMembers, const int* numParInZone, int* slot_out) {
+  TRACE("d3q19_pool_admit");
   if (!p || !ip || !fp || !f || !u || !slot_out) return D3Q19_EINVAL;
   POOL_LOCK(p);
   d3q19_options o;
@@ -1563,6 +1582,7 @@ static int pool_enqueue(d3q19_pool* p, int nsteps) {
 }
 
 extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
+  TRACE("d3q19_pool_advance");
   if (!p) return D3Q19_EINVAL;
   POOL_LOCK(p);
   if (nsteps <= 0 || nsteps % p->period != 0)
@@ -1607,6 +1627,7 @@ extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
 
 extern "C" int d3q19_pool_mean_stress(d3q19_pool* p, double* stress_xz, double* shear_rate, double* eff_viscosity,
                                       int* status) {
+  TRACE("d3q19_pool_mean_stress");
   if (!p || !stress_xz || !status) return D3Q19_EINVAL;
   POOL_LOCK(p);
   cudaSetDevice(p->dev);
@@ -1699,12 +1720,14 @@ static int release_slot(d3q19_pool* p, int slot) {
 }
 
 extern "C" int d3q19_pool_release(d3q19_pool* p, int slot) {
+  TRACE("d3q19_pool_release");
   if (!p) return D3Q19_EINVAL;
   POOL_LOCK(p);
   return release_slot(p, slot);
 }
 
 extern "C" int d3q19_pool_evict(d3q19_pool* p, int slot, void* buf, size_t bytes) {
+  TRACE("d3q19_pool_evict");
   if (!p) return D3Q19_EINVAL;
   POOL_LOCK(p);
   if (slot < 0 || slot >= p->max_slots || !p->slot[slot]) return D3Q19_EINVAL;
@@ -1717,6 +1740,7 @@ extern "C" int d3q19_pool_evict(d3q19_pool* p, int slot, void* buf, size_t bytes
 
 extern "C" int d3q19_pool_readmit(d3q19_pool* p, const int_param_struct* ip, const flp_param_struct* fp,
                                   const d3q19_options* opt, const void* buf, size_t bytes, int* slot_out) {
+  TRACE("d3q19_pool_readmit");
   if (!p || !ip || !fp || !buf || !slot_out) return D3Q19_EINVAL;
   POOL_LOCK(p);
   if (bytes < sizeof(CkptHeader)) return pfail(p, D3Q19_EINVAL, "not a checkpoint");
