@@ -82,3 +82,21 @@ def test_program_outputs_fast_arithmetic(name):
         assert a.shape == b.shape, fn
         assert np.abs(a - b).max() <= 5e-6, fn
     shutil.rmtree(d)
+
+
+def test_program_stops_on_a_malformed_sphere_file():
+    # Exit status 1 and the reference's message, before the device is used
+    # for the run (the reference exits in the same place).
+    d = tempfile.mkdtemp(prefix="d3q19prog_")
+    os.makedirs(os.path.join(d, "matlab_postproc"))
+    os.makedirs(os.path.join(d, "unit_sphere_partitions"))
+    with open(os.path.join(d, "unit_sphere_partitions", "unit_sphere_partition_256.txt"), "w") as fh:
+        fh.write("0,0,1\n" * 40)  # truncated
+    kw = dict(iterations=5, total_lattice_size=(24, 24, 24), boundary_conditions_xyz=(0, 0, 1), num_particles=1,
+              particle_diameter=8.0, initial_particle_distribution=3, initial_particle_buffer=11.0,
+              domain_decomposition=(1, 1, 1))
+    with open(os.path.join(d, "input_file.txt"), "w") as fh:
+        fh.write(d3.keywords_text(kw))
+    p = subprocess.run([os.path.join(PKG, "bin", "d3q19_b200")], cwd=d, capture_output=True, text=True, timeout=120)
+    assert p.returncode == 1 and "malformed coordinates read in sphere discretization" in p.stderr
+    assert not os.path.exists(os.path.join(d, "velocity_field_final.txt"))

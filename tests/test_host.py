@@ -206,3 +206,46 @@ def test_output_writers_match_reference_files(name, usp_dir):
                                    kin.ctypes.data_as(C.c_void_p), fh, n_last)
         libc.fclose(fh)
         assert open(vid).read() == last
+
+
+def _sphere_config(d=8.0):
+    kw = dict(total_lattice_size=(24, 24, 24), boundary_conditions_xyz=(0, 0, 1), num_particles=1,
+              particle_diameter=d, initial_particle_distribution=3, initial_particle_buffer=11.0,
+              domain_decomposition=(1, 1, 1))
+    return d3.parse_config(d3.keywords_text(kw))
+
+
+@pytest.mark.parametrize("defect", ["truncated", "off_sphere", "not_numbers"])
+def test_malformed_partition_file_is_rejected(defect):
+    # The reference prints and exits on a malformed sphere file
+    # (D3Q19-OpenCL.c:598-601); here the host set-up returns an error the
+    # caller sees, before any device work.
+    cfg = _sphere_config()
+    P = 256  # 2^ceil(log2(pi d^2)) for d = 8
+    d = tempfile.mkdtemp(prefix="d3q19usp_")
+    os.makedirs(os.path.join(d, "unit_sphere_partitions"))
+    pts = np.zeros((P, 3))
+    pts[:, 2] = 1.0
+    lines = [f"{x:.5g},{y:.5g},{z:.5g}" for x, y, z in pts]
+    if defect == "truncated":
+        lines = lines[:100]
+    elif defect == "off_sphere":
+        lines[37] = "1.2,0,0"
+    else:
+        lines[5] = "a,b,c"
+    with open(os.path.join(d, "unit_sphere_partitions", f"unit_sphere_partition_{P}.txt"), "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    with pytest.raises(d3.D3Q19Error, match="malformed"):
+        d3.HostState(cfg, data_dir=d)
+
+
+def test_well_formed_partition_file_is_used():
+    cfg = _sphere_config()
+    P = 256
+    d = tempfile.mkdtemp(prefix="d3q19usp_")
+    os.makedirs(os.path.join(d, "unit_sphere_partitions"))
+    with open(os.path.join(d, "unit_sphere_partitions", f"unit_sphere_partition_{P}.txt"), "w") as fh:
+        fh.write("0,0,1\n" * P)
+    hs = d3.HostState(cfg, data_dir=d)
+    sp = hs.spherePoints.reshape(P, 4)
+    assert np.allclose(sp[:, :3], [0.0, 0.0, 4.0])  # unit points scaled by d/2
