@@ -1,6 +1,8 @@
 """Build recipe of the native parts, in-tree:
 
   lib/libd3q19_b200.so   CUDA kernels + C ABI (nvcc, sm_100a, static cudart)
+  lib/libd3q19_b200_checked.so   the same with -DD3Q19_BOUNDS_CHECK=1 (device index
+                         checks that record D3Q19_EBOUNDS instead of faulting)
   lib/libd3q19_host.so   C host routines (parser, initial state, outputs)
   bin/d3q19_b200         the simulation program (drop-in for the reference's binary)
 
@@ -16,6 +18,7 @@ REPO = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "lib")
 BIN = os.path.join(PKG, "bin")
 CUDA_LIB = os.path.join(LIB, "libd3q19_b200.so")
+CHECKED_LIB = os.path.join(LIB, "libd3q19_b200_checked.so")
 HOST_LIB = os.path.join(LIB, "libd3q19_host.so")
 MAIN = os.path.join(BIN, "d3q19_b200")
 
@@ -44,25 +47,35 @@ def _run(cmd):
     subprocess.check_call(cmd)
 
 
-def build(force: bool = False, verbose_ptxas: bool = False):
+def _cuda_lib(target, objdir, defines, force, verbose_ptxas):
+    if not (force or _stale(target, CU_SRC + CU_HDR + [__file__])):
+        return
+    os.makedirs(objdir, exist_ok=True)
+    objs, cmds = [], []
+    for src in CU_SRC:
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"] + defines + ["-c", "-o", obj,
+                                                                                                   src]
+        if os.path.basename(src) in NO_CONTRACT:
+            cmd.insert(1, "--fmad=false")
+        if verbose_ptxas:
+            cmd.insert(1, "-Xptxas=-v")
+        cmds.append(cmd)
+        objs.append(obj)
+    # The translation units are independent: compile them concurrently.
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(cmds)) as ex:
+        list(ex.map(_run, cmds))
+    _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", target] + objs)
+
+
+def build(force: bool = False, verbose_ptxas: bool = False, checked: bool = True):
     os.makedirs(LIB, exist_ok=True)
     os.makedirs(BIN, exist_ok=True)
-    if force or _stale(CUDA_LIB, CU_SRC + CU_HDR + [__file__]):
-        os.makedirs(OBJ, exist_ok=True)
-        objs, cmds = [], []
-        for src in CU_SRC:
-            obj = os.path.join(OBJ, os.path.basename(src) + ".o")
-            cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-c", "-o", obj, src]
-            if os.path.basename(src) in NO_CONTRACT:
-                cmd.insert(1, "--fmad=false")
-            if verbose_ptxas:
-                cmd.insert(1, "-Xptxas=-v")
-            cmds.append(cmd)
-            objs.append(obj)
-        # The translation units are independent: compile them concurrently.
-        with concurrent.futures.ThreadPoolExecutor(max_workers=len(cmds)) as ex:
-            list(ex.map(_run, cmds))
-        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", CUDA_LIB] + objs)
+    jobs = [(CUDA_LIB, OBJ, [])]
+    if checked:
+        jobs.append((CHECKED_LIB, os.path.join(OBJ, "checked"), ["-DD3Q19_BOUNDS_CHECK=1"]))
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        list(ex.map(lambda j: _cuda_lib(*j, force, verbose_ptxas), jobs))
     if force or _stale(HOST_LIB, HOST_SRC + HOST_HDR + [__file__]):
         _run(["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-Wall", "-Wno-unused-result", "-o", HOST_LIB]
              + HOST_SRC + ["-lm"])

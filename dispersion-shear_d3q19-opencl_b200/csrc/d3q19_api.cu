@@ -14,6 +14,7 @@
 #include <limits>
 #include <map>
 #include <mutex>
+#include <string>
 #include <tuple>
 #include <vector>
 
@@ -568,6 +569,7 @@ static FluidArgs fluid_args(const d3q19_ctx* c, int t, int cur) {
   fa.tiles.list = c->tile_list;
   fa.tiles.mrec = c->mrec;
   fa.tiles.fmax = c->fmax;
+  fa.tiles.markers = (long long)c->ppar.np * c->ppar.P;
   fa.has_ibm = c->ppar.np > 0;
   fa.err = c->err;
   fa.clamps = c->clamps;
@@ -593,6 +595,7 @@ static ParticleArgs particle_args(const d3q19_ctx* c, int t, int pcur) {
   pa.tiles.list = c->tile_list;
   pa.tiles.mrec = c->mrec;
   pa.tiles.fmax = c->fmax;
+  pa.tiles.markers = (long long)c->ppar.np * c->ppar.P;
   pa.znd = c->znd;
   pa.parsZone = c->parsZone;
   pa.zoneMembers = c->zoneMembers;
@@ -805,6 +808,8 @@ static int device_errors(d3q19_ctx* c) {
   if (c->sticky & ERR_TILE_OVERFLOW)
     return fail(c, D3Q19_EOVERFLOW, "a lattice tile received more than %d IBM markers; raise ibm_tile_capacity",
                 c->tile_cap);
+  if (c->sticky & ERR_BOUNDS)
+    return fail(c, D3Q19_EBOUNDS, "an index check of the bounds-checked build failed (the access was skipped)");
   if (c->sticky & (ERR_NONFINITE | ERR_FIXED_RANGE))
     return fail(c, D3Q19_ENUMERIC, "non-finite or out-of-range density, velocity or marker position on the device");
   if (c->sticky & ERR_ZONE_RANGE) return fail(c, D3Q19_ENUMERIC, "sphere position outside the zone grid");
@@ -899,6 +904,7 @@ extern "C" int d3q19_read_spread_force(d3q19_ctx* c, float* gpf0) {
     tl.list = c->tile_list;
     tl.mrec = c->mrec;
     tl.fmax = c->fmax;
+    tl.markers = (long long)c->ppar.np * c->ppar.P;
     if (c->opt.arithmetic == 1)
       CUDA_TRY(c, launch_spread_field_exact(c->g, tl, c->ip.MaxSurfPointsPerNode, (float*)c->scratch, c->err,
                                             c->stream));
@@ -1138,6 +1144,7 @@ extern "C" int d3q19_read_spread_force_static(d3q19_ctx* c, float* gpf0) {
     tl.list = c->tile_list;
     tl.mrec = c->mrec;
     tl.fmax = c->fmax;
+    tl.markers = (long long)c->ppar.np * c->ppar.P;
     if (c->opt.arithmetic == 1)
       CUDA_TRY(c, launch_spread_field_exact(c->g, tl, c->ip.MaxSurfPointsPerNode, field, c->err, c->stream));
     else
@@ -1163,39 +1170,82 @@ struct CkptHeader {
 struct CkptBlock {
   void* ptr;
   size_t bytes;
+  const char* name;
 };
 std::vector<CkptBlock> ckpt_blocks(d3q19_ctx* c) {
   const long long NC = c->g.NC;
   std::vector<CkptBlock> b;
-  b.push_back({c->f[c->cur], (size_t)storage_bytes(c->opt.storage) * 19 * NC});
-  b.push_back({c->u, sizeof(float) * 3 * NC});
-  b.push_back({c->tau, sizeof(float) * NC});
-  if (c->tau64) b.push_back({c->tau64, sizeof(double) * NC});
+  b.push_back({c->f[c->cur], (size_t)storage_bytes(c->opt.storage) * 19 * NC, "f"});
+  b.push_back({c->u, sizeof(float) * 3 * NC, "u"});
+  b.push_back({c->tau, sizeof(float) * NC, "tau"});
+  if (c->tau64) b.push_back({c->tau64, sizeof(double) * NC, "tau64"});
   const long long np = c->ppar.np;
   if (np > 0) {
     const long long M = np * c->ppar.P, nfa = c->ppar.nfa;
-    b.push_back({c->kin[c->pcur], sizeof(float4) * 4 * np});
-    b.push_back({c->pf[c->pcur], sizeof(float4) * 2 * np});
-    b.push_back({c->pff[c->pcur], sizeof(float4) * 2 * np * nfa});
+    b.push_back({c->kin[c->pcur], sizeof(float4) * 4 * np, "kin"});
+    b.push_back({c->pf[c->pcur], sizeof(float4) * 2 * np, "pf"});
+    b.push_back({c->pff[c->pcur], sizeof(float4) * 2 * np * nfa, "pff"});
     if (c->kin64[0]) {
-      b.push_back({c->kin64[c->pcur], sizeof(double) * 16 * np});
-      b.push_back({c->pff64[c->pcur], sizeof(double) * 8 * np * nfa});
+      b.push_back({c->kin64[c->pcur], sizeof(double) * 16 * np, "kin64"});
+      b.push_back({c->pff64[c->pcur], sizeof(double) * 8 * np * nfa, "pff64"});
     }
-    b.push_back({c->sphere, sizeof(float4) * c->ppar.P});
-    b.push_back({c->mrec, sizeof(float4) * 2 * M});
-    b.push_back({c->tile_count, sizeof(int) * c->ntiles});
-    b.push_back({c->tile_list, sizeof(int) * c->ntiles * c->tile_cap});
-    b.push_back({c->fmax, sizeof(unsigned) * 2});
+    b.push_back({c->sphere, sizeof(float4) * c->ppar.P, "sphere"});
+    b.push_back({c->mrec, sizeof(float4) * 2 * M, "mrec"});
+    b.push_back({c->tile_count, sizeof(int) * c->ntiles, "tile_count"});
+    b.push_back({c->tile_list, sizeof(int) * c->ntiles * c->tile_cap, "tile_list"});
+    b.push_back({c->fmax, sizeof(unsigned) * 2, "fmax"});
     const long long Z = c->nzones;
-    b.push_back({c->znd, sizeof(int) * 28 * Z});
-    b.push_back({c->parsZone, sizeof(int) * np});
-    b.push_back({c->zoneMembers, sizeof(int) * Z * np});
-    b.push_back({c->numParInZone, sizeof(int) * Z});
-    b.push_back({c->revStart, sizeof(int) * (Z + 1)});
-    b.push_back({c->revList, sizeof(int) * 27 * Z});
-    b.push_back({c->zoneOf, sizeof(int) * np});
+    b.push_back({c->znd, sizeof(int) * 28 * Z, "znd"});
+    b.push_back({c->parsZone, sizeof(int) * np, "parsZone"});
+    b.push_back({c->zoneMembers, sizeof(int) * Z * np, "zoneMembers"});
+    b.push_back({c->numParInZone, sizeof(int) * Z, "numParInZone"});
+    b.push_back({c->revStart, sizeof(int) * (Z + 1), "revStart"});
+    b.push_back({c->revList, sizeof(int) * 27 * Z, "revList"});
+    b.push_back({c->zoneOf, sizeof(int) * np, "zoneOf"});
   }
   return b;
+}
+
+// The integer tables of a checkpoint index device arrays: before they are
+// uploaded, every entry the kernels follow must lie inside its array (a
+// damaged buffer is refused instead of making a kernel read out of bounds).
+const char* ckpt_tables_invalid(d3q19_ctx* c, const char* data) {
+  const long long np = c->ppar.np;
+  if (np == 0) return nullptr;
+  const long long M = np * c->ppar.P, Z = c->nzones, cap = c->tile_cap;
+  const int *tile_count = nullptr, *tile_list = nullptr, *znd = nullptr, *members = nullptr, *nin = nullptr,
+            *rstart = nullptr, *rlist = nullptr;
+  size_t off = 0;
+  for (const auto& b : ckpt_blocks(c)) {
+    const int* q = reinterpret_cast<const int*>(data + off);
+    const std::string n = b.name;
+    if (n == "tile_count") tile_count = q;
+    else if (n == "tile_list") tile_list = q;
+    else if (n == "znd") znd = q;
+    else if (n == "zoneMembers") members = q;
+    else if (n == "numParInZone") nin = q;
+    else if (n == "revStart") rstart = q;
+    else if (n == "revList") rlist = q;
+    off += b.bytes;
+  }
+  for (long long T = 0; T < c->ntiles; T++) {
+    if (tile_count[T] < 0) return "tile count";
+    const long long n = std::min<long long>(tile_count[T], cap);
+    for (long long j = 0; j < n; j++)
+      if (tile_list[T * cap + j] < 0 || tile_list[T * cap + j] >= M) return "tile list entry";
+  }
+  for (long long z = 0; z < Z; z++) {
+    if (znd[28 * z] < 0 || znd[28 * z] > 27) return "zone neighbour count";
+    if (nin[z] < 0 || nin[z] > np) return "zone member count";
+    for (long long j = 0; j < nin[z]; j++)
+      if (members[z * np + j] < 0 || members[z * np + j] >= np) return "zone member";
+  }
+  if (rstart[0] != 0 || rstart[Z] > 27 * Z) return "reverse zone table";
+  for (long long z = 0; z < Z; z++)
+    if (rstart[z + 1] < rstart[z]) return "reverse zone table";
+  for (long long r = 0; r < rstart[Z]; r++)
+    if (rlist[r] < 0 || rlist[r] >= Z) return "reverse zone entry";
+  return nullptr;
 }
 }  // namespace
 
@@ -1259,6 +1309,8 @@ extern "C" int d3q19_restore(d3q19_ctx* c, const void* buf, size_t bytes) {
   size_t need = 0;
   d3q19_checkpoint_bytes(c, &need);
   if (bytes < need) return fail(c, D3Q19_EINVAL, "checkpoint truncated (%zu of %zu bytes)", bytes, need);
+  if (const char* bad = ckpt_tables_invalid(c, static_cast<const char*>(buf) + sizeof(h)))
+    return fail(c, D3Q19_EINVAL, "checkpoint damaged: %s out of range", bad);
   cudaSetDevice(c->dev);
   if (int rc = join_side(c)) return rc;
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -1673,7 +1725,8 @@ extern "C" int d3q19_pool_mean_stress(d3q19_pool* p, double* stress_xz, double* 
     const int Nz = c->g.Nz;
     const unsigned e = (unsigned)h[off[s] + 5 * (size_t)Nz];
     c->sticky |= e;
-    status[s] = (c->sticky & ERR_TILE_OVERFLOW) ? D3Q19_EOVERFLOW
+    status[s] = (c->sticky & ERR_BOUNDS)          ? D3Q19_EBOUNDS
+                : (c->sticky & ERR_TILE_OVERFLOW) ? D3Q19_EOVERFLOW
                 : (c->sticky & (ERR_NONFINITE | ERR_FIXED_RANGE | ERR_ZONE_RANGE)) ? D3Q19_ENUMERIC
                                                                                      : 0;
     double gs = 0.0, ts = 0.0;

@@ -33,6 +33,7 @@ constexpr unsigned ERR_TILE_OVERFLOW = 1u;
 constexpr unsigned ERR_NONFINITE = 2u;
 constexpr unsigned ERR_ZONE_RANGE = 4u;
 constexpr unsigned ERR_FIXED_RANGE = 8u;
+constexpr unsigned ERR_BOUNDS = 16u;  // an index check of the bounds-checked build failed (access skipped)
 
 struct Geom {
   int Nx, Ny, Nz;
@@ -66,6 +67,7 @@ struct TileLists {
   int* list;           // [ntiles * cap] marker ids
   const float4* mrec;  // [2 * markers]
   unsigned* fmax;      // [2] float bits of the largest |marker force| per step parity
+  long long markers;   // marker records in mrec (checked by the bounds-checked build)
 };
 
 struct FluidArgs {

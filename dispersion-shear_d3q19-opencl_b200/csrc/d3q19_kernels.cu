@@ -39,6 +39,24 @@
 
 namespace d3q19 {
 
+// Bounds-checked build (-DD3Q19_BOUNDS_CHECK=1): the data-dependent indices
+// of the kernels (pull sources, marker ids read from the tile lists, the
+// interpolation stencil, zone and sphere ids of the contact search) are
+// checked; an index outside its array sets ERR_BOUNDS and the access is
+// skipped.  In the default build the check compiles to nothing.
+#ifndef D3Q19_BOUNDS_CHECK
+#define D3Q19_BOUNDS_CHECK 0
+#endif
+__device__ __forceinline__ bool out_of_bounds(long long idx, long long n, unsigned* err) {
+#if D3Q19_BOUNDS_CHECK
+  if ((unsigned long long)idx >= (unsigned long long)n) {
+    atomicOr(err, ERR_BOUNDS);
+    return true;
+  }
+#endif
+  return false;
+}
+
 // D3Q19 velocities in the reference's order (D3Q19-OpenCL.c:9-13), as
 // compile-time expressions of q so fully unrolled loops fold them.
 #define CXQ(q) (((q) == 1 || (q) == 7 || (q) == 8 || (q) == 9 || (q) == 10) ? 1 : \
@@ -249,12 +267,16 @@ __device__ __forceinline__ R compute_tau(const FluidParams& p, R srt, bool& clam
 // 32-bit int (N_C < 2^31 is checked when the context is created).
 template <typename ST, typename R>
 __device__ __forceinline__ void gather(R (&f)[19], const ST* __restrict__ fin, long long NC, int i, int dxm,
-                                       int dxp, int dym, int dyp, int dzm, int dzp) {
+                                       int dxp, int dym, int dyp, int dzm, int dzp, unsigned* err) {
 #pragma unroll
   for (int q = 0; q < 19; q++) {
     const int cx = CXQ(q), cy = CYQ(q), cz = CZQ(q);
     const int src = i + (cx == 1 ? dxm : (cx == -1 ? dxp : 0)) + (cy == 1 ? dym : (cy == -1 ? dyp : 0)) +
                     (cz == 1 ? dzm : (cz == -1 ? dzp : 0));
+    if (out_of_bounds(src, NC, err)) {
+      f[q] = wq<R>(q);
+      continue;
+    }
     f[q] = Stored<ST>::load(fin + q * NC + src, wq<R>(q));
   }
 }
@@ -514,7 +536,7 @@ template <typename R = float>
 __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& tl, long long T, int n, int X0,
                                 int Y0, int Z0, int tid, int k, int first_id, unsigned* err) {
   float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
-  if (tid < n) {  // issued before the clear so that the round trip overlaps it
+  if (tid < n && !out_of_bounds(first_id, tl.markers, err)) {  // issued before the clear: the round trip overlaps it
     ma = tl.mrec[2 * (long long)first_id];
     mb = tl.mrec[2 * (long long)first_id + 1];
   }
@@ -528,6 +550,7 @@ __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& t
     float4 a = ma, b = mb;
     if (j != tid) {
       const int m = tl.list[T * tl.cap + j];
+      if (out_of_bounds(m, tl.markers, err)) continue;
       a = tl.mrec[2 * (long long)m];
       b = tl.mrec[2 * (long long)m + 1];
     }
@@ -692,6 +715,7 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
     const int z = Z0 + 2 * threadIdx.z + zz;
     if (!inxy || z < 1 || z > g.Nz - 2) continue;
     const int i = x + g.Nx * (y + g.Ny * z);
+    if (out_of_bounds(i, NC, a.err)) continue;
     R f[19];
     if (first) {
 #pragma unroll
@@ -702,13 +726,13 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
       const int dxp = x == g.Nx - 2 ? -(g.Nx - 3) : 1;
       const int dym = (y == 1 ? g.Ny - 3 : -1) * g.Nx;
       const int dyp = (y == g.Ny - 2 ? -(g.Ny - 3) : 1) * g.Nx;
-      gather(f, fin, NC, i, dxm, dxp, dym, dyp, -Nxy, Nxy);
+      gather(f, fin, NC, i, dxm, dxp, dym, dyp, -Nxy, Nxy, a.err);
       if (z == 1) velocity_bc<2, 0>(f, a.p.velLower);
       else if (z == g.Nz - 2) velocity_bc<2, 1>(f, a.p.velUpper);
     } else {
       int dxm, dxp, dym, dyp, dzm, dzp;
       neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
-      gather(f, fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp);
+      gather(f, fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp, a.err);
       boundaries(f, g, a.p, x, y, z);
     }
     const R gx = R(a.p.g[0]) + (zz ? sg[1][0] : sg[0][0]);
@@ -792,7 +816,7 @@ __global__ void materialize_f_kernel(const FluidArgs a, float* __restrict__ out)
     int dxm, dxp, dym, dyp, dzm, dzp;
     neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
     typename RealOf<ST>::type f[19];
-    gather(f, static_cast<const ST*>(a.fin), NC, i, dxm, dxp, dym, dyp, dzm, dzp);
+    gather(f, static_cast<const ST*>(a.fin), NC, i, dxm, dxp, dym, dyp, dzm, dzp, a.err);
     boundaries(f, g, a.p, x, y, z);
 #pragma unroll
     for (int q = 0; q < 19; q++) out[q * NC + i] = (float)f[q];
@@ -1090,6 +1114,7 @@ __device__ __forceinline__ void particle_group(const ParticleArgs& a, const int 
         for (int j = 0; j < 8; j++) {
           const long long i =
               (x0 + sh[j][0]) + (long long)g.Nx * ((y0 + sh[j][1]) + (long long)g.Ny * (z0 + sh[j][2]));
+          if (out_of_bounds(i, g.NC, a.err)) continue;
           // GPU_program.cl:193-195, without contraction.
           ux = __fadd_rn(ux, __fmul_rn(w[j], a.u[i]));
           uy = __fadd_rn(uy, __fmul_rn(w[j], a.u[i + g.NC]));
@@ -1261,6 +1286,7 @@ __device__ __forceinline__ void particle_group_f64(const ParticleArgs& a, const 
       for (int j = 0; j < 8; j++) {
         const long long i =
             (x0 + sh[j][0]) + (long long)g.Nx * ((y0 + sh[j][1]) + (long long)g.Ny * (z0 + sh[j][2]));
+        if (out_of_bounds(i, g.NC, a.err)) continue;
         ux += w[j] * a.u[i];
         uy += w[j] * a.u[i + g.NC];
         uz += w[j] * a.u[i + 2 * g.NC];
@@ -1347,8 +1373,9 @@ __device__ __forceinline__ void contact_sphere(const ParticleArgs& a, const int 
         const int zid = a.znd[28 * pz + t];
         if (zid < 0 || zid >= nzones) continue;
         for (int j = 0; j < a.numParInZone[zid]; j++) {
+          if (out_of_bounds(j, np, a.err)) break;
           const int pj = a.zoneMembers[zid * np + j];
-          if (!(pi > pj)) continue;
+          if (out_of_bounds(pj, np, a.err) || !(pi > pj)) continue;
           const Kin kj = load_kin(a.kin_new, pj, np);
           float4 e;
           float fm;
@@ -1389,8 +1416,9 @@ __device__ __forceinline__ void contact_sphere(const ParticleArgs& a, const int 
       if (zid < 0 || zid >= nzones) continue;  // zone ids past the grid name no zone
       const int cnt = a.numParInZone[zid];
       for (int j = 0; j < cnt; j++) {
+        if (out_of_bounds(j, np, a.err)) break;
         const int pj = a.zoneMembers[zid * np + j];
-        if (!(pi > pj)) continue;
+        if (out_of_bounds(pj, np, a.err) || !(pi > pj)) continue;
         const Kin kj = load_kin(a.kin_new, pj, np);
         float4 e;
         float fm;
@@ -1399,10 +1427,12 @@ __device__ __forceinline__ void contact_sphere(const ParticleArgs& a, const int 
     }
     for (int r = a.revStart[pz] + lane; r < a.revStart[pz + 1]; r += 32) {
       const int Y = a.revList[r];
+      if (out_of_bounds(Y, nzones, a.err)) continue;
       const int cnt = a.numParInZone[Y];
       for (int j = 0; j < cnt; j++) {
+        if (out_of_bounds(j, np, a.err)) break;
         const int pk = a.zoneMembers[Y * np + j];
-        if (!(pk > pi)) continue;
+        if (out_of_bounds(pk, np, a.err) || !(pk > pi)) continue;
         const Kin kk = load_kin(a.kin_new, pk, np);
         float4 e;
         float fm;

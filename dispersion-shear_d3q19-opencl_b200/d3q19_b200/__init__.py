@@ -14,13 +14,16 @@ import numpy as np
 
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIBDIR = os.path.join(PKG, "lib")
-CUDA_LIB = os.path.join(LIBDIR, "libd3q19_b200.so")
+# D3Q19_BOUNDS_CHECK=1 in the environment selects the bounds-checked build
+# (device index checks that report D3Q19_EBOUNDS instead of faulting).
+CUDA_LIB = os.path.join(LIBDIR, "libd3q19_b200_checked.so" if os.environ.get("D3Q19_BOUNDS_CHECK") == "1"
+                        else "libd3q19_b200.so")
 HOST_LIB = os.path.join(LIBDIR, "libd3q19_host.so")
 
 # Largest lattice (N_C nodes) d3q19_read_spread_force_static accepts.
 STATIC_SPREAD_MAX_CELLS = 262144
 STATUS = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ENODEV", -5: "EOVERFLOW", -6: "ENUMERIC",
-          -7: "ESTATE", -8: "EBUSY"}
+          -7: "ESTATE", -8: "EBUSY", -9: "EBOUNDS"}
 EBUSY = -8
 
 _INT_FIELDS = [

@@ -75,7 +75,9 @@ enum d3q19_status {
   D3Q19_EOVERFLOW = -5, /* a lattice tile received more IBM markers than its list holds */
   D3Q19_ENUMERIC = -6,  /* non-finite density or velocity detected on the device */
   D3Q19_ESTATE = -7,    /* call out of order (e.g. step before the lattice is written) */
-  D3Q19_EBUSY = -8      /* the pool has no free slot or HBM budget for the request right now */
+  D3Q19_EBUSY = -8,     /* the pool has no free slot or HBM budget for the request right now */
+  D3Q19_EBOUNDS = -9    /* library built with D3Q19_BOUNDS_CHECK: a device index fell outside its array (the
+                           access was skipped); no counterpart in the reference */
 };
 
 /* Options with no counterpart in the reference's parameter structs.  A

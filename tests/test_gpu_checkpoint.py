@@ -169,3 +169,59 @@ def test_pool_readmit_refusals():
         pool.readmit(odd)
     assert pool.readmit(ev) is not None
     pool.close()
+
+
+def _ckpt_layout(ck):
+    """Byte offsets of the integer tables of an FP32 checkpoint with spheres
+    (header: magic, version, storage, p64, arithmetic, NC, ntiles, np, nfa, P,
+    cap, nzones, f_state, last_t, sticky, clamps)."""
+    import struct
+
+    (_, _, storage, p64, arith, NC, ntiles, npar, nfa, P, cap, Z, _, _, _, _) = struct.unpack_from(
+        "<8s4i2q5i3iq", ck.tobytes(), 0)
+    assert storage == 0 and p64 == 0 and arith == 0
+    M = npar * P
+    sizes = [("f", 4 * 19 * NC), ("u", 12 * NC), ("tau", 4 * NC), ("kin", 64 * npar), ("pf", 32 * npar),
+             ("pff", 32 * npar * nfa), ("sphere", 16 * P), ("mrec", 32 * M), ("tile_count", 4 * ntiles),
+             ("tile_list", 4 * ntiles * cap), ("fmax", 8), ("znd", 4 * 28 * Z), ("parsZone", 4 * npar),
+             ("zoneMembers", 4 * Z * npar), ("numParInZone", 4 * Z), ("revStart", 4 * (Z + 1)),
+             ("revList", 4 * 27 * Z), ("zoneOf", 4 * npar)]
+    off, out = 80, {}
+    for name, n in sizes:
+        out[name] = off
+        off += n
+    assert off == len(ck)
+    return out, dict(np=npar, Z=Z, cap=cap, ntiles=ntiles)
+
+
+@pytest.mark.parametrize("damage", ["zone_member", "tile_list", "reverse_table", "neighbour_count"])
+def test_restore_refuses_damaged_tables(damage):
+    # A checkpoint's integer tables index device arrays: a damaged entry is
+    # refused on the host before anything is uploaded.
+    hs = sv.host_state(SUSP)
+    a = d3.Simulation.from_host_state(hs)
+    a.run(1, 10)
+    ck = a.checkpoint()
+    off, dims = _ckpt_layout(ck)
+    ints = lambda name, n: np.frombuffer(ck, np.int32, count=n, offset=off[name])
+    bad = ck.copy()
+    view = lambda name, n: bad[off[name]:off[name] + 4 * n].view(np.int32)  # noqa: E731  (writable)
+    if damage == "zone_member":
+        nin = ints("numParInZone", dims["Z"])
+        z = int(np.argmax(nin > 0))
+        view("zoneMembers", dims["Z"] * dims["np"])[z * dims["np"]] = dims["np"] + 7
+    elif damage == "tile_list":
+        cnt = ints("tile_count", dims["ntiles"])
+        T = int(np.argmax(cnt > 0))
+        assert cnt[T] > 0
+        view("tile_list", dims["ntiles"] * dims["cap"])[T * dims["cap"]] = -3
+    elif damage == "reverse_table":
+        view("revStart", dims["Z"] + 1)[dims["Z"]] = 27 * dims["Z"] + 5
+    else:
+        view("znd", 28 * dims["Z"])[0] = 99
+    with pytest.raises(d3.D3Q19Error, match="damaged"):
+        a.restore(bad)
+    a.restore(ck)  # the intact one still restores
+    a.run(11, 5)
+    a.synchronize()
+    a.close()
