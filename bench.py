@@ -13,6 +13,7 @@ Metric: MLUPS = interior nodes x steps / s / 1e6, summed over GPUs (each GPU
 runs an independent replica: weak scaling, no collective on the data path).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--storage fp32|fp16|bf16] [--inplace]
 
 Other modes (--workload, one GPU, one JSON line each): powerlaw-128-fluid and
 couette-sphere-64 (the same line for the fluid alone and the 64^3 single
@@ -195,7 +196,7 @@ def ncu_traffic(workload, storage="fp32"):
         return None
 
 
-def setup(workload, device, storage="fp32"):
+def setup(workload, device, storage="fp32", inplace=False):
     import numpy as np  # noqa: F401
 
     import d3q19_b200 as d3
@@ -204,7 +205,8 @@ def setup(workload, device, storage="fp32"):
     hs = d3.HostState(cfg, data_dir=os.getcwd())
     hs.options.device = device
     hs.options.storage = STORAGE[storage][0]
-    sim = d3.Simulation.from_host_state(hs, device=device, storage=STORAGE[storage][0])
+    hs.options.inplace = int(inplace)
+    sim = d3.Simulation.from_host_state(hs, device=device, storage=STORAGE[storage][0], inplace=int(inplace))
     return d3, hs, sim
 
 
@@ -256,7 +258,7 @@ def run_ours(args, rank, world, local_rank, dist):
     import torch
 
     torch.cuda.set_device(local_rank)
-    d3, hs, sim = setup(args.workload, local_rank, args.storage)
+    d3, hs, sim = setup(args.workload, local_rank, args.storage, args.inplace)
     bytes_per_node = STORAGE[args.storage][1]
     ip = hs.cfg.ip
     interior = (ip.LatticeSize[0] - 2) * (ip.LatticeSize[1] - 2) * (ip.LatticeSize[2] - 2)
@@ -348,9 +350,11 @@ def run_ours(args, rank, world, local_rank, dist):
         "config": {"workload": args.workload, "description": DESCRIPTION[args.workload],
                    "lattice": list(ip.LatticeSize), "interior_nodes": interior, "spheres": ip.NumParticles,
                    "markers_per_sphere": ip.PointsPerParticle, "parallelism": f"replicas x{world}",
-                   "l2": l2_note(ip, bytes_per_node)},
+                   "l2": l2_note(ip, bytes_per_node),
+                   "distribution_buffers": 1 if args.inplace else 2},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": ncu_traffic(args.workload, args.storage),
+                     "frac": round(achieved / peak, 4),
+                     "traffic": None if args.inplace else ncu_traffic(args.workload, args.storage),
                      "kernel": "fluid_step_kernel", "bytes_per_node": bytes_per_node,
                      "kernel_ms": round(fluid_avg, 5), "particle_kernel_ms": round(part_avg, 5),
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
@@ -733,6 +737,8 @@ def main():
                                                                                            "casson-precision"])
     ap.add_argument("--requests", type=int, default=128, help="served-sweep: number of requests")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--inplace", action="store_true",
+                    help="one distribution buffer updated in place (AA pattern) instead of two")
     ap.add_argument("--storage", default="fp32", choices=sorted(STORAGE),
                     help="distribution storage: fp32 (the reference's), or 16-bit shifted")
     args = ap.parse_args()

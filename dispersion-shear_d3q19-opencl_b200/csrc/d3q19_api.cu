@@ -175,6 +175,9 @@ static int validate(const int_param_struct* ip, const flp_param_struct* fp, cons
     return fail(nullptr, D3Q19_EINVAL, "more than 1 pair of faces with velocity boundaries (D3Q19-OpenCL.c:103)");
   if (o->collision < 0 || o->collision > 1) return fail(nullptr, D3Q19_EINVAL, "collision must be 0 or 1");
   if (o->arithmetic < 0 || o->arithmetic > 2) return fail(nullptr, D3Q19_EINVAL, "arithmetic must be 0, 1 or 2");
+  if (o->inplace != 0 && o->inplace != 1) return fail(nullptr, D3Q19_EINVAL, "inplace must be 0 or 1");
+  if (o->inplace && o->arithmetic == 1)
+    return fail(nullptr, D3Q19_EINVAL, "in-place streaming is not available with the reference's evaluation order");
   if (o->arithmetic == 2 && (o->collision != 0 || o->storage != 0))
     return fail(nullptr, D3Q19_EINVAL, "the FP64 build runs the reference's MRT on FP64 distributions only");
   if (o->arithmetic == 1 && o->collision != 0)
@@ -316,7 +319,9 @@ static int create_ctx(const int_param_struct* ip, const flp_param_struct* fp, co
 
   const long long NC = g.NC;
   const size_t fbytes = (size_t)storage_bytes(o.storage) * 19 * NC;
-  if ((rc = dalloc(c, (char**)&c->f[0], fbytes)) || (rc = dalloc(c, (char**)&c->f[1], fbytes)) ||
+  // In place: one buffer, under both names (fin == fout).
+  if ((rc = dalloc(c, (char**)&c->f[0], fbytes)) ||
+      (o.inplace ? (c->f[1] = c->f[0], 0) : (rc = dalloc(c, (char**)&c->f[1], fbytes))) ||
       (rc = dalloc(c, &c->u, 3 * NC)) ||
       (rc = dalloc(c, &c->tau, NC)) || (rc = dalloc(c, &c->err, 1)) || (rc = dalloc(c, &c->clamps, 1)) ||
       (rc = dalloc(c, &c->pstats, 5LL * g.Nz)) || (o.arithmetic == 2 && (rc = dalloc(c, &c->tau64, NC)))) {
@@ -373,6 +378,7 @@ static int create_ctx(const int_param_struct* ip, const flp_param_struct* fp, co
 extern "C" int d3q19_write_lattice(d3q19_ctx* c, const float* f, const float* u, const float* tau_lb) {
   if (!c || !f || !u) return D3Q19_EINVAL;
   cudaSetDevice(c->dev);
+  if (c->opt.inplace) c->cur = 0;  // the uploaded layout is the one even steps read
   const long long NC = c->g.NC;
   if (c->opt.storage == STORE_F32) {
     CUDA_TRY(c, cudaMemcpyAsync(c->f[c->cur], f, sizeof(float) * 19 * NC, cudaMemcpyHostToDevice, c->stream));
@@ -573,6 +579,7 @@ static FluidArgs fluid_args(const d3q19_ctx* c, int t, int cur) {
   fa.has_ibm = c->ppar.np > 0;
   fa.err = c->err;
   fa.clamps = c->clamps;
+  fa.inplace = c->opt.inplace ? (cur == 0 ? 1 : 2) : 0;  // even steps read buffer parity 0
   return fa;
 }
 
@@ -885,6 +892,7 @@ extern "C" int d3q19_read_f(d3q19_ctx* c, float* f) {
   fa.g = c->g;
   fa.p = c->fpar;
   fa.fin = c->f[c->cur];
+  fa.inplace = c->opt.inplace ? (c->cur == 0 ? 1 : 2) : 0;
   CUDA_TRY(c, cudaMemsetAsync(c->scratch, 0, sizeof(float) * 19 * NC, c->stream));
   CUDA_TRY(c, launch_materialize_f(fa, c->opt.storage, (float*)c->scratch, c->stream));
   return readback(c, f, (const float*)c->scratch, 19 * NC);
@@ -1063,6 +1071,7 @@ extern "C" int d3q19_destroy(d3q19_ctx* c) {
   if (c->side) cudaStreamSynchronize(c->side);
   for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
   drop_events(c);
+  if (c->f[1] == c->f[0]) c->f[1] = nullptr;  // in place: one buffer
   void* ptrs[] = {c->f[0], c->f[1], c->u, c->tau, c->kin[0], c->kin[1], c->pff[0], c->pff[1], c->pf[0], c->pf[1],
                   c->sphere, c->mrec, c->tile_count, c->fmax, c->tile_list, c->znd, c->parsZone, c->zoneMembers,
                   c->numParInZone, c->revStart, c->revList, c->zoneOf, c->err, c->clamps, c->pstats, c->scratch,
@@ -1164,6 +1173,7 @@ struct CkptHeader {
   long long NC, ntiles;
   int np, nfa, P, cap, nzones;
   int f_state, last_t, sticky;
+  int inplace, phase;  // in place: the buffer parity the next step reads (the layout of f)
   long long clamps;
 };
 // The device blocks of a checkpoint in order: {pointer, bytes}.
@@ -1269,7 +1279,7 @@ extern "C" int d3q19_checkpoint(d3q19_ctx* c, void* buf, size_t bytes) {
   CkptHeader h;
   memset(&h, 0, sizeof(h));
   memcpy(h.magic, "D3Q19CK", 8);
-  h.version = 1;
+  h.version = 2;
   h.storage = c->opt.storage;
   h.p64 = c->kin64[0] != nullptr;
   h.arithmetic = c->opt.arithmetic;
@@ -1283,6 +1293,8 @@ extern "C" int d3q19_checkpoint(d3q19_ctx* c, void* buf, size_t bytes) {
   h.f_state = c->f_state;
   h.last_t = c->last_t;
   h.sticky = (int)c->sticky;
+  h.inplace = c->opt.inplace;
+  h.phase = c->cur;
   unsigned long long cl = 0;
   char* p = static_cast<char*>(buf) + sizeof(h);
   CUDA_TRY(c, cudaMemcpyAsync(&cl, c->clamps, sizeof(cl), cudaMemcpyDeviceToHost, c->stream));
@@ -1301,10 +1313,10 @@ extern "C" int d3q19_restore(d3q19_ctx* c, const void* buf, size_t bytes) {
   if (!c || !buf || bytes < sizeof(CkptHeader)) return D3Q19_EINVAL;
   CkptHeader h;
   memcpy(&h, buf, sizeof(h));
-  if (memcmp(h.magic, "D3Q19CK", 8) != 0 || h.version != 1) return fail(c, D3Q19_EINVAL, "not a checkpoint");
+  if (memcmp(h.magic, "D3Q19CK", 8) != 0 || h.version != 2) return fail(c, D3Q19_EINVAL, "not a checkpoint");
   if (h.storage != c->opt.storage || h.p64 != (c->kin64[0] != nullptr) || h.arithmetic != c->opt.arithmetic ||
       h.NC != c->g.NC || h.ntiles != c->ntiles || h.np != c->ppar.np || h.nfa != c->ppar.nfa || h.P != c->ppar.P ||
-      h.cap != c->tile_cap || h.nzones != c->nzones)
+      h.cap != c->tile_cap || h.nzones != c->nzones || h.inplace != c->opt.inplace)
     return fail(c, D3Q19_EINVAL, "checkpoint of a context with other parameters");
   size_t need = 0;
   d3q19_checkpoint_bytes(c, &need);
@@ -1325,6 +1337,7 @@ extern "C" int d3q19_restore(d3q19_ctx* c, const void* buf, size_t bytes) {
   CUDA_TRY(c, cudaMemcpyAsync(c->err, &e, sizeof(e), cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));  // the host values above go out of scope
   c->sticky = e;
+  if (c->opt.inplace) c->cur = h.phase;  // the buffer's layout
   c->f_state = h.f_state;
   c->last_t = h.last_t;
   c->have_particles = c->have_zones = true;
@@ -1349,7 +1362,7 @@ extern "C" int d3q19_context_bytes(const int_param_struct* ip, const d3q19_optio
   const long long NC = (long long)ip->LatticeSize[0] * ip->LatticeSize[1] * ip->LatticeSize[2];
   const long long ntiles = (long long)((ip->LatticeSize[0] + TILE_X - 1) / TILE_X) *
                            ((ip->LatticeSize[1] + TILE_Y - 1) / TILE_Y) * ((ip->LatticeSize[2] + TILE_Z - 1) / TILE_Z);
-  size_t b = 2 * round_alloc((size_t)storage_bytes(o.storage) * 19 * NC) + round_alloc(12 * (size_t)NC) +
+  size_t b = (o.inplace ? 1 : 2) * round_alloc((size_t)storage_bytes(o.storage) * 19 * NC) + round_alloc(12 * (size_t)NC) +
              round_alloc(4 * (size_t)NC) + 3 * 512 + round_alloc(40 * (size_t)ip->LatticeSize[2]) +
              (o.arithmetic == 2 ? round_alloc(8 * (size_t)NC) : 0);
   const long long np = ip->NumParticles;
@@ -1489,8 +1502,8 @@ static int pool_place(d3q19_pool* p, const int_param_struct* ip, const d3q19_opt
   o.device = p->dev;
   if (o.storage != p->storage) return pfail(p, D3Q19_EINVAL, "storage %d differs from the pool's %d", o.storage,
                                             p->storage);
-  if (o.arithmetic != 0 || o.collision != 0 || o.particle_precision != 0)
-    return pfail(p, D3Q19_EINVAL, "the pool runs the fast FP32 arithmetic with the reference's MRT only");
+  if (o.arithmetic != 0 || o.collision != 0 || o.particle_precision != 0 || o.inplace != 0)
+    return pfail(p, D3Q19_EINVAL, "the pool runs the fast FP32 arithmetic with the reference's MRT and two buffers only");
   if (ip->BoundaryConds[0] != 0 || ip->BoundaryConds[1] != 0 || ip->BoundaryConds[2] != 1 ||
       o.tangential_vel_bc[0] || o.tangential_vel_bc[1] || o.tangential_vel_bc[2])
     return pfail(p, D3Q19_EINVAL, "the pool runs shear cells: periodic x and y, velocity walls on z");

@@ -85,6 +85,9 @@ struct FluidArgs {
   int has_ibm;
   unsigned* err;
   unsigned long long* clamps;
+  // 0: two buffers.  In place (fin == fout): 1 = the next step is an even
+  // step (cells read and written at the node), 2 = an odd step.
+  int inplace;
 };
 
 struct ParticleParams {

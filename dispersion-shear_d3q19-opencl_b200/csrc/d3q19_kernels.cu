@@ -281,6 +281,31 @@ __device__ __forceinline__ void gather(R (&f)[19], const ST* __restrict__ fin, l
   }
 }
 
+// The odd step of the in-place (AA) layout: population q of node i is the
+// post-collision value the upwind neighbour i - c_q stored, with the
+// direction reversed, in its cell opp(q).
+template <typename ST, typename R>
+__device__ __forceinline__ void gather_reversed(R (&f)[19], const ST* __restrict__ fin, long long NC, int i, int dxm,
+                                                int dxp, int dym, int dyp, int dzm, int dzp, unsigned* err) {
+#pragma unroll
+  for (int q = 0; q < 19; q++) {
+    const int cx = CXQ(q), cy = CYQ(q), cz = CZQ(q);
+    const int src = i + (cx == 1 ? dxm : (cx == -1 ? dxp : 0)) + (cy == 1 ? dym : (cy == -1 ? dyp : 0)) +
+                    (cz == 1 ? dzm : (cz == -1 ? dzp : 0));
+    if (out_of_bounds(src, NC, err)) {
+      f[q] = wq<R>(q);
+      continue;
+    }
+    f[q] = Stored<ST>::load(fin + OPPQ(q) * NC + src, wq<R>(q));
+  }
+}
+
+// Offsets to the neighbours x-1, x+1, y-1, y+1, z-1, z+1 of an interior node
+// for a boundary layout (wrapped on periodic axes).
+template <int BC>
+__device__ __forceinline__ void layout_deltas(const Geom& g, int x, int y, int z, int& dxm, int& dxp, int& dym,
+                                              int& dyp, int& dzm, int& dzp);
+
 // Index deltas to the upwind neighbours of node (x,y,z).
 __device__ __forceinline__ void neighbour_deltas(const Geom& g, int x, int y, int z, int& dxm, int& dxp, int& dym,
                                                  int& dyp, int& dzm, int& dzp) {
@@ -291,6 +316,22 @@ __device__ __forceinline__ void neighbour_deltas(const Geom& g, int x, int y, in
   dyp = ((g.periodic[1] && y == g.Ny - 2) ? -(g.Ny - 3) : 1) * g.Nx;
   dzm = ((g.periodic[2] && z == 1) ? g.Nz - 3 : -1) * Nxy;
   dzp = ((g.periodic[2] && z == g.Nz - 2) ? -(g.Nz - 3) : 1) * Nxy;
+}
+
+template <int BC>
+__device__ __forceinline__ void layout_deltas(const Geom& g, int x, int y, int z, int& dxm, int& dxp, int& dym,
+                                              int& dyp, int& dzm, int& dzp) {
+  if (BC == 1) {  // BC_ZWALL: periodic x and y, walls on z
+    const int Nxy = g.Nx * g.Ny;
+    dxm = x == 1 ? g.Nx - 3 : -1;
+    dxp = x == g.Nx - 2 ? -(g.Nx - 3) : 1;
+    dym = (y == 1 ? g.Ny - 3 : -1) * g.Nx;
+    dyp = (y == g.Ny - 2 ? -(g.Ny - 3) : 1) * g.Nx;
+    dzm = -Nxy;
+    dzp = Nxy;
+  } else {
+    neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
+  }
 }
 
 // Boundary rebuild after the gather: the wall plane of the wall axis, then
@@ -665,7 +706,12 @@ __host__ __device__ constexpr size_t fluid_smem_bytes(bool ibm) { return ibm ? s
 // One collide-stream pass over a 32x4x4 tile; each thread takes two
 // consecutive z-planes.  first != 0: the stored state is the reference's
 // post-stream buffer (after an upload), read in place without streaming.
-template <int COLL, int VISC, int BC, typename ST>
+// AA: 0 = two buffers (pull from fin, write fout); 1 and 2 = the even and
+// odd steps of the in-place layout (fin == fout).  Even: read the node's own
+// cells, write them back with the directions reversed.  Odd: pull the
+// reversed cells of the upwind neighbours, push to the downwind ones.
+// Every cell is read and then written by one thread only.
+template <int COLL, int VISC, int BC, typename ST, int AA = 0>
 __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, const int bx, const int by,
                                            const int bz, SpreadSmem& sm) {
   const ST* __restrict__ fin = static_cast<const ST*>(a.fin);
@@ -717,23 +763,44 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
     const int i = x + g.Nx * (y + g.Ny * z);
     if (out_of_bounds(i, NC, a.err)) continue;
     R f[19];
-    if (first) {
+    if (AA == 0) {
+      if (first) {
 #pragma unroll
-      for (int q = 0; q < 19; q++) f[q] = Stored<ST>::load(fin + q * NC + i, wq<R>(q));
-    } else if (BC == BC_ZWALL) {
-      const int Nxy = g.Nx * g.Ny;
-      const int dxm = x == 1 ? g.Nx - 3 : -1;
-      const int dxp = x == g.Nx - 2 ? -(g.Nx - 3) : 1;
-      const int dym = (y == 1 ? g.Ny - 3 : -1) * g.Nx;
-      const int dyp = (y == g.Ny - 2 ? -(g.Ny - 3) : 1) * g.Nx;
-      gather(f, fin, NC, i, dxm, dxp, dym, dyp, -Nxy, Nxy, a.err);
-      if (z == 1) velocity_bc<2, 0>(f, a.p.velLower);
-      else if (z == g.Nz - 2) velocity_bc<2, 1>(f, a.p.velUpper);
+        for (int q = 0; q < 19; q++) f[q] = Stored<ST>::load(fin + q * NC + i, wq<R>(q));
+      } else if (BC == BC_ZWALL) {
+        const int Nxy = g.Nx * g.Ny;
+        const int dxm0 = x == 1 ? g.Nx - 3 : -1;
+        const int dxp0 = x == g.Nx - 2 ? -(g.Nx - 3) : 1;
+        const int dym0 = (y == 1 ? g.Ny - 3 : -1) * g.Nx;
+        const int dyp0 = (y == g.Ny - 2 ? -(g.Ny - 3) : 1) * g.Nx;
+        gather(f, fin, NC, i, dxm0, dxp0, dym0, dyp0, -Nxy, Nxy, a.err);
+        if (z == 1) velocity_bc<2, 0>(f, a.p.velLower);
+        else if (z == g.Nz - 2) velocity_bc<2, 1>(f, a.p.velUpper);
+      } else {
+        int dxm0, dxp0, dym0, dyp0, dzm0, dzp0;
+        neighbour_deltas(g, x, y, z, dxm0, dxp0, dym0, dyp0, dzm0, dzp0);
+        gather(f, fin, NC, i, dxm0, dxp0, dym0, dyp0, dzm0, dzp0, a.err);
+        boundaries(f, g, a.p, x, y, z);
+      }
     } else {
-      int dxm, dxp, dym, dyp, dzm, dzp;
-      neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
-      gather(f, fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp, a.err);
-      boundaries(f, g, a.p, x, y, z);
+      if (first || AA == 1) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) f[q] = Stored<ST>::load(fin + q * NC + i, wq<R>(q));
+      } else {
+        int dxm, dxp, dym, dyp, dzm, dzp;
+        layout_deltas<BC>(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
+        gather_reversed(f, fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp, a.err);
+      }
+      // The uploaded state is the reference's buffer after its boundary
+      // kernels; every later step rebuilds the wall unknowns.
+      if (!first) {
+        if (BC == BC_ZWALL) {
+          if (z == 1) velocity_bc<2, 0>(f, a.p.velLower);
+          else if (z == g.Nz - 2) velocity_bc<2, 1>(f, a.p.velUpper);
+        } else {
+          boundaries(f, g, a.p, x, y, z);
+        }
+      }
     }
     const R gx = R(a.p.g[0]) + (zz ? sg[1][0] : sg[0][0]);
     const R gy = R(a.p.g[1]) + (zz ? sg[1][1] : sg[0][1]);
@@ -762,20 +829,37 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
       a.tau[i] = (float)tau;
       nclamp += clamped ? 1 : 0;
     }
+    if (AA == 1) {
 #pragma unroll
-    for (int q = 0; q < 19; q++) Stored<ST>::store(fout + q * NC + i, f[q], wq<R>(q));
+      for (int q = 0; q < 19; q++) Stored<ST>::store(fout + OPPQ(q) * NC + i, f[q], wq<R>(q));
+    } else if (AA == 2) {
+      // Recomputed here rather than kept live across the collision.
+      int dxm, dxp, dym, dyp, dzm, dzp;
+      layout_deltas<BC>(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
+#pragma unroll
+      for (int q = 0; q < 19; q++) {
+        const int cx = CXQ(q), cy = CYQ(q), cz = CZQ(q);
+        const int dst = i + (cx == 1 ? dxp : (cx == -1 ? dxm : 0)) + (cy == 1 ? dyp : (cy == -1 ? dym : 0)) +
+                        (cz == 1 ? dzp : (cz == -1 ? dzm : 0));
+        if (out_of_bounds(dst, NC, a.err)) continue;
+        Stored<ST>::store(fout + q * NC + dst, f[q], wq<R>(q));
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 19; q++) Stored<ST>::store(fout + q * NC + i, f[q], wq<R>(q));
+    }
   }
   if (var && nclamp) atomicAdd(a.clamps, (unsigned long long)nclamp);
 }
 
-template <int COLL, int VISC, int BC, typename ST>
+template <int COLL, int VISC, int BC, typename ST, int AA>
 __global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4   ? FLUID_MIN_BLOCKS_F32
                                                  : sizeof(ST) == 8 ? 2
                                                                    : FLUID_MIN_BLOCKS)
     fluid_step_kernel(const FluidArgs a, const int first) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  fluid_tile<COLL, VISC, BC, ST>(a, first, blockIdx.x, blockIdx.y, blockIdx.z,
-                                 *reinterpret_cast<SpreadSmem*>(smem_raw));
+  fluid_tile<COLL, VISC, BC, ST, AA>(a, first, blockIdx.x, blockIdx.y, blockIdx.z,
+                                     *reinterpret_cast<SpreadSmem*>(smem_raw));
 }
 
 // The collide-stream pass of many independent lattices in one persistent
@@ -816,7 +900,18 @@ __global__ void materialize_f_kernel(const FluidArgs a, float* __restrict__ out)
     int dxm, dxp, dym, dyp, dzm, dzp;
     neighbour_deltas(g, x, y, z, dxm, dxp, dym, dyp, dzm, dzp);
     typename RealOf<ST>::type f[19];
-    gather(f, static_cast<const ST*>(a.fin), NC, i, dxm, dxp, dym, dyp, dzm, dzp, a.err);
+    const ST* fin = static_cast<const ST*>(a.fin);
+    // The next step's inputs: in place after an odd in-place step (the
+    // neighbours pushed them), reversed in the upwind cells after an even
+    // one, pulled from the other buffer otherwise.
+    if (a.inplace == 1) {
+#pragma unroll
+      for (int q = 0; q < 19; q++) f[q] = Stored<ST>::load(fin + q * NC + i, wq<typename RealOf<ST>::type>(q));
+    } else if (a.inplace == 2) {
+      gather_reversed(f, fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp, a.err);
+    } else {
+      gather(f, fin, NC, i, dxm, dxp, dym, dyp, dzm, dzp, a.err);
+    }
     boundaries(f, g, a.p, x, y, z);
 #pragma unroll
     for (int q = 0; q < 19; q++) out[q * NC + i] = (float)f[q];
@@ -1611,7 +1706,9 @@ static cudaError_t launch_fluid_t(const FluidArgs& a, bool first, cudaStream_t s
   dim3 block(TILE_X, TILE_Y, 2);
   dim3 grid(a.g.ntx, a.g.nty, a.g.ntz);
   const size_t smem = fluid_smem_bytes(a.has_ibm != 0);
-  fluid_step_kernel<COLL, VISC, BC, ST><<<grid, block, smem, s>>>(a, first ? 1 : 0);
+  if (a.inplace == 1) fluid_step_kernel<COLL, VISC, BC, ST, 1><<<grid, block, smem, s>>>(a, first ? 1 : 0);
+  else if (a.inplace == 2) fluid_step_kernel<COLL, VISC, BC, ST, 2><<<grid, block, smem, s>>>(a, first ? 1 : 0);
+  else fluid_step_kernel<COLL, VISC, BC, ST, 0><<<grid, block, smem, s>>>(a, first ? 1 : 0);
   return cudaGetLastError();
 }
 

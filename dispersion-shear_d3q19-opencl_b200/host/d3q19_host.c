@@ -82,6 +82,7 @@ static const keyword_t KEYWORDS[] = {
     {"particle_precision", T_INT, HPO(ParticlePrecision), "0"},
     {"reference_arithmetic", T_INT, HPO(Arithmetic), "0"},
     {"fp64_build", T_INT, HPO(Fp64Build), "0"},
+    {"inplace_streaming", T_INT, HPO(Inplace), "0"},
 };
 #define NKEYWORDS ((int)(sizeof(KEYWORDS) / sizeof(KEYWORDS[0])))
 
@@ -716,5 +717,6 @@ void d3q19h_options(const d3q19h_config* cfg, d3q19_options* o) {
   o->tau_max = cfg->hp.TauMax;
   o->tau_min = cfg->hp.TauMin;
   o->arithmetic = cfg->hp.Fp64Build ? 2 : cfg->hp.Arithmetic;
+  o->inplace = cfg->hp.Inplace;
   o->casson_reg = cfg->hp.CassonReg;
 }

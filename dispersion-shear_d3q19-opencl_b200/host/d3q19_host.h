@@ -50,6 +50,7 @@ typedef struct {
   int ParticlePrecision;      /* particle_precision: 0 fp32 (reference), 1 fp64 */
   int Arithmetic;             /* reference_arithmetic: 1 = the reference's evaluation order */
   int Fp64Build;              /* fp64_build: 1 = the FP64 build of the fast kernels (arithmetic 2) */
+  int Inplace;                /* inplace_streaming: 1 = one distribution buffer (AA pattern) */
 } d3q19h_host_params;
 
 typedef struct {

@@ -133,6 +133,13 @@ typedef struct {
    * local tau, spread smoothing, and particle_precision 1): the oracle the
    * FP32 and 16-bit forms are measured against; the reference's MRT only. */
   int arithmetic;
+  /* 0: two distribution buffers, as the reference's fA/fB.  1: one buffer
+   * updated in place (AA pattern): even steps read a node's own cells and
+   * write them back with the directions reversed, odd steps pull from and
+   * push to the neighbours.  Half the distribution memory, the same results
+   * bit for bit.  Not with arithmetic 1, not in a lattice pool.  No
+   * counterpart in the reference. */
+  int inplace;
 } d3q19_options;
 
 typedef struct {

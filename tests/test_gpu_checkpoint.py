@@ -174,11 +174,11 @@ def test_pool_readmit_refusals():
 def _ckpt_layout(ck):
     """Byte offsets of the integer tables of an FP32 checkpoint with spheres
     (header: magic, version, storage, p64, arithmetic, NC, ntiles, np, nfa, P,
-    cap, nzones, f_state, last_t, sticky, clamps)."""
+    cap, nzones, f_state, last_t, sticky, inplace, phase, clamps)."""
     import struct
 
-    (_, _, storage, p64, arith, NC, ntiles, npar, nfa, P, cap, Z, _, _, _, _) = struct.unpack_from(
-        "<8s4i2q5i3iq", ck.tobytes(), 0)
+    (_, _, storage, p64, arith, NC, ntiles, npar, nfa, P, cap, Z, _, _, _, _, _, _) = struct.unpack_from(
+        "<8s4i2q5i3i2iq", ck.tobytes(), 0)
     assert storage == 0 and p64 == 0 and arith == 0
     M = npar * P
     sizes = [("f", 4 * 19 * NC), ("u", 12 * NC), ("tau", 4 * NC), ("kin", 64 * npar), ("pf", 32 * npar),
@@ -186,7 +186,7 @@ def _ckpt_layout(ck):
              ("tile_list", 4 * ntiles * cap), ("fmax", 8), ("znd", 4 * 28 * Z), ("parsZone", 4 * npar),
              ("zoneMembers", 4 * Z * npar), ("numParInZone", 4 * Z), ("revStart", 4 * (Z + 1)),
              ("revList", 4 * 27 * Z), ("zoneOf", 4 * npar)]
-    off, out = 80, {}
+    off, out = 88, {}
     for name, n in sizes:
         out[name] = off
         off += n
