@@ -1409,9 +1409,14 @@ struct d3q19_pool {
   int part_threads = 128;
   bool dirty = true;
   int fblocks = 0, pblocks = 0, cblocks = 0;
+  int sm_count = 0;
+  // Layout of the members (d3q19_options.inplace) while the pool has any; -1
+  // when empty.  In place, every member sits at buffer parity 0 between
+  // chunks, so step j of a chunk is an even step for all when j is even.
+  int inplace = -1;
   double* d_stats = nullptr;  // per-member plane sums and error words (d3q19_pool_mean_stress)
   size_t stats_cap = 0;
-  std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;  // (steps, fblocks, pblocks, cblocks)
+  std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> graphs;  // (steps, fblocks, pblocks, cblocks, inplace)
   long long steps = 0;
   // Every d3q19_pool_* call holds it: the pool may be driven from several
   // host threads (its members are not stepped outside these calls).
@@ -1465,6 +1470,7 @@ extern "C" int d3q19_pool_create(int device, int storage, int rebuild_freq, int 
   p->slot_steps.assign(max_slots, 0);
   // Persistent grids: blocks per SM the kernels' register and shared memory
   // bounds allow (the autotuner may lower them).
+  p->sm_count = pr.multiProcessorCount;
   p->fblocks = pr.multiProcessorCount * (storage == STORE_F32 ? 5 : 4);
   p->pblocks = pr.multiProcessorCount * 4;
   p->cblocks = pr.multiProcessorCount * 4;
@@ -1502,8 +1508,10 @@ static int pool_place(d3q19_pool* p, const int_param_struct* ip, const d3q19_opt
   o.device = p->dev;
   if (o.storage != p->storage) return pfail(p, D3Q19_EINVAL, "storage %d differs from the pool's %d", o.storage,
                                             p->storage);
-  if (o.arithmetic != 0 || o.collision != 0 || o.particle_precision != 0 || o.inplace != 0)
-    return pfail(p, D3Q19_EINVAL, "the pool runs the fast FP32 arithmetic with the reference's MRT and two buffers only");
+  if (o.arithmetic != 0 || o.collision != 0 || o.particle_precision != 0)
+    return pfail(p, D3Q19_EINVAL, "the pool runs the fast FP32 arithmetic with the reference's MRT only");
+  if (p->inplace >= 0 && o.inplace != p->inplace)
+    return pfail(p, D3Q19_EINVAL, "inplace %d differs from the pool members' %d", o.inplace, p->inplace);
   if (ip->BoundaryConds[0] != 0 || ip->BoundaryConds[1] != 0 || ip->BoundaryConds[2] != 1 ||
       o.tangential_vel_bc[0] || o.tangential_vel_bc[1] || o.tangential_vel_bc[2])
     return pfail(p, D3Q19_EINVAL, "the pool runs shear cells: periodic x and y, velocity walls on z");
@@ -1552,6 +1560,11 @@ extern "C" int d3q19_pool_admit(d3q19_pool* p, const int_param_struct* ip, const
     d3q19_destroy(c);
     return rc;
   }
+  if (c->opt.inplace && c->cur != 0) {  // cannot happen: the warm-up is an even number of steps
+    d3q19_destroy(c);
+    return pfail(p, D3Q19_ESTATE, "in-place member out of phase");
+  }
+  p->inplace = c->opt.inplace;
   p->slot[s] = c;
   p->slot_bytes[s] = bytes;
   p->slot_steps[s] = p->period;
@@ -1637,7 +1650,11 @@ static int pool_enqueue(d3q19_pool* p, int nsteps) {
   const int2* cw = p->d_work + 2 * p->work_cap;
   for (int j = 0; j < nsteps; j++) {
     const int par = j & 1;
-    POOL_TRY(p, launch_fluid_batch(p->d_fargs, fw, p->d_counts + 0, par, p->storage, p->fblocks, p->stream));
+    // In place, the FP32 kernels run 4 blocks/SM: a larger persistent grid
+    // would only add a second wave.
+    const int aa = p->inplace == 1 ? (par == 0 ? 1 : 2) : 0;
+    const int fb = aa && p->storage == STORE_F32 ? std::min(p->fblocks, 4 * p->sm_count) : p->fblocks;
+    POOL_TRY(p, launch_fluid_batch(p->d_fargs, fw, p->d_counts + 0, par, p->storage, aa, fb, p->stream));
     POOL_TRY(p, launch_particle_batch(p->d_pargs, pw, p->d_counts + 1, par, p->part_threads, p->pblocks, p->stream));
     POOL_TRY(p, launch_contact_batch(p->d_pargs, cw, p->d_counts + 2, par, p->cblocks, p->stream));
     if ((j + 1) % p->rebuild == 0)
@@ -1661,7 +1678,7 @@ extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
     }
   if (p->dirty)
     if (int rc = pool_upload(p)) return rc;
-  auto key = std::make_tuple(nsteps, p->fblocks, p->pblocks, p->cblocks);
+  auto key = std::make_tuple(nsteps, p->fblocks, p->pblocks, p->cblocks, p->inplace);
   auto it = p->graphs.find(key);
   if (it == p->graphs.end()) {
     cudaGraph_t graph;
@@ -1782,6 +1799,9 @@ static int release_slot(d3q19_pool* p, int slot) {
   p->slot_bytes[slot] = 0;
   p->slot_steps[slot] = 0;
   p->dirty = true;
+  bool empty = true;
+  for (auto* m : p->slot) empty = empty && !m;
+  if (empty) p->inplace = -1;
   return 0;
 }
 
@@ -1828,6 +1848,11 @@ extern "C" int d3q19_pool_readmit(d3q19_pool* p, const int_param_struct* ip, con
     d3q19_destroy(c);
     return rc;
   }
+  if (c->opt.inplace && c->cur != 0) {
+    d3q19_destroy(c);
+    return pfail(p, D3Q19_EINVAL, "in-place checkpoint at an odd phase");
+  }
+  p->inplace = c->opt.inplace;
   p->slot[s] = c;
   p->slot_bytes[s] = need;
   p->slot_steps[s] = h.last_t;

@@ -170,8 +170,9 @@ cudaError_t launch_zones(const ZoneArgs& a, cudaStream_t s);
 // Batched passes over many lattices (the lattice pool): persistent grids of
 // `blocks` CTAs over packed work lists {slot, tile | group | sphere} whose
 // lengths are read on the device; per-lattice arguments slots[2*s + parity].
+// inplace: 0 two buffers, 1 / 2 the even / odd in-place step of every member.
 cudaError_t launch_fluid_batch(const FluidArgs* slots, const int2* work, const int* nwork, int parity, int storage,
-                               int blocks, cudaStream_t s);
+                               int inplace, int blocks, cudaStream_t s);
 cudaError_t launch_particle_batch(const ParticleArgs* slots, const int2* work, const int* nwork, int parity,
                                   int threads, int blocks, cudaStream_t s);
 cudaError_t launch_contact_batch(const ParticleArgs* slots, const int2* work, const int* nwork, int parity,

@@ -872,8 +872,11 @@ __global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4   ? (AA ? FLUID
 // work[k] = {slot, tile} (*nwork items).  slots[2*s + parity] holds lattice
 // s's arguments for steps of that buffer parity.  The reference's MRT rates,
 // periodic x/y with z walls, and each lattice's own viscosity law.
-template <typename ST>
-__global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? FLUID_MIN_BLOCKS_F32 : FLUID_MIN_BLOCKS)
+// AA: the pool's layout for this step (every member of a pool shares it and
+// sits at the same phase).
+template <typename ST, int AA>
+__global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? (AA ? FLUID_MIN_BLOCKS_AA_F32 : FLUID_MIN_BLOCKS_F32)
+                                                                 : FLUID_MIN_BLOCKS)
     fluid_batch_kernel(const FluidArgs* __restrict__ slots, const int2* __restrict__ work,
                        const int* __restrict__ nwork, const int parity) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -884,7 +887,7 @@ __global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? FLUID_MIN_BLO
     const FluidArgs& a = slots[2 * it.x + parity];
     const int ntx = a.g.ntx, nty = a.g.nty;
     const int bx = it.y % ntx, by = (it.y / ntx) % nty, bz = it.y / (ntx * nty);
-    fluid_tile<0, -1, BC_ZWALL, ST>(a, 0, bx, by, bz, sm);
+    fluid_tile<0, -1, BC_ZWALL, ST, AA>(a, 0, bx, by, bz, sm);
     __syncthreads();  // the spread halo is reused by the next item
   }
 }
@@ -1798,14 +1801,21 @@ cudaError_t launch_contacts(const ParticleArgs& a, cudaStream_t s) {
 
 // Batched passes (the lattice pool): fixed persistent grids, the work list
 // lengths live on the device so one captured sequence serves any mix.
-cudaError_t launch_fluid_batch(const FluidArgs* slots, const int2* work, const int* nwork, int parity, int storage,
-                               int blocks, cudaStream_t s) {
+template <typename ST>
+static void fluid_batch_aa(const FluidArgs* slots, const int2* work, const int* nwork, int parity, int inplace,
+                           int blocks, size_t smem, cudaStream_t s) {
   const dim3 block(TILE_X, TILE_Y, 2);
+  if (inplace == 1) fluid_batch_kernel<ST, 1><<<blocks, block, smem, s>>>(slots, work, nwork, parity);
+  else if (inplace == 2) fluid_batch_kernel<ST, 2><<<blocks, block, smem, s>>>(slots, work, nwork, parity);
+  else fluid_batch_kernel<ST, 0><<<blocks, block, smem, s>>>(slots, work, nwork, parity);
+}
+
+cudaError_t launch_fluid_batch(const FluidArgs* slots, const int2* work, const int* nwork, int parity, int storage,
+                               int inplace, int blocks, cudaStream_t s) {
   const size_t smem = fluid_smem_bytes(true);
-  if (storage == STORE_F16) fluid_batch_kernel<__half><<<blocks, block, smem, s>>>(slots, work, nwork, parity);
-  else if (storage == STORE_BF16)
-    fluid_batch_kernel<__nv_bfloat16><<<blocks, block, smem, s>>>(slots, work, nwork, parity);
-  else fluid_batch_kernel<float><<<blocks, block, smem, s>>>(slots, work, nwork, parity);
+  if (storage == STORE_F16) fluid_batch_aa<__half>(slots, work, nwork, parity, inplace, blocks, smem, s);
+  else if (storage == STORE_BF16) fluid_batch_aa<__nv_bfloat16>(slots, work, nwork, parity, inplace, blocks, smem, s);
+  else fluid_batch_aa<float>(slots, work, nwork, parity, inplace, blocks, smem, s);
   return cudaGetLastError();
 }
 

@@ -475,7 +475,7 @@ class Pool:
     batched persistent kernels (d3q19_pool_* of the C ABI)."""
 
     def __init__(self, device: int = 0, storage: int = 0, rebuild_freq: int = 10, max_slots: int = 256,
-                 hbm_budget: int = 64 << 30):
+                 hbm_budget: int = 64 << 30, inplace: bool = False):
         self.lib = cuda_lib()
         h = C.c_void_p()
         rc = self.lib.d3q19_pool_create(device, storage, rebuild_freq, max_slots, hbm_budget, C.byref(h))
@@ -483,6 +483,7 @@ class Pool:
             raise D3Q19Error(f"d3q19_pool_create: {STATUS.get(rc, rc)}: {self.lib.d3q19_pool_last_error(None).decode()}")
         self.h = h
         self.storage = storage
+        self.inplace = int(inplace)  # members keep one distribution buffer (AA pattern)
         self.max_slots = max_slots
         self.rebuild_freq = rebuild_freq
         self.period = 2 // math.gcd(2, rebuild_freq) * rebuild_freq
@@ -498,6 +499,7 @@ class Pool:
         opt = Options.from_buffer_copy(bytes(hs.options))
         opt.storage = self.storage
         opt.rebuild_freq = self.rebuild_freq
+        opt.inplace = self.inplace
         for k, v in option_overrides.items():
             setattr(opt, k, v)
         slot = C.c_int(-1)
@@ -524,6 +526,7 @@ class Pool:
         opt = Options.from_buffer_copy(bytes(hs.options))
         opt.storage = self.storage
         opt.rebuild_freq = self.rebuild_freq
+        opt.inplace = self.inplace
         for k, v in option_overrides.items():
             setattr(opt, k, v)
         used, budget, n = self.usage()

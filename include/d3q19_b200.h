@@ -137,8 +137,8 @@ typedef struct {
    * updated in place (AA pattern): even steps read a node's own cells and
    * write them back with the directions reversed, odd steps pull from and
    * push to the neighbours.  Half the distribution memory, the same results
-   * bit for bit.  Not with arithmetic 1, not in a lattice pool.  No
-   * counterpart in the reference. */
+   * bit for bit.  Not with arithmetic 1.  The members of a lattice pool share
+   * one layout.  No counterpart in the reference. */
   int inplace;
 } d3q19_options;
 

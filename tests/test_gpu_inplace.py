@@ -101,8 +101,12 @@ def test_inplace_memory_and_refusals():
         sim_from_golden(g, CASES["contacts"], inplace=1, arithmetic=1)
     from d3q19_b200 import serving as sv
 
+    # The members of a pool share one layout.
     pool = d3.Pool(storage=0, max_slots=2)
     req = sv.ShearRequest(rid=0, edge=(32, 32, 32), phi=0.1, model="newtonian", wall_speed=0.02, seed=3)
+    s = pool.admit(sv.host_state(req))
     with pytest.raises(d3.D3Q19Error, match="EINVAL"):
         pool.admit(sv.host_state(req), inplace=1)
+    pool.release(s)
+    assert pool.admit(sv.host_state(req), inplace=1) is not None  # an empty pool takes either
     pool.close()

@@ -39,8 +39,8 @@ def bits_equal(a, b):
         assert x.shape == y.shape and np.array_equal(x.view(np.uint8), y.view(np.uint8)), k
 
 
-def alone(req, storage, schedule):
-    pool = d3.Pool(storage=storage, max_slots=4)
+def alone(req, storage, schedule, inplace=False):
+    pool = d3.Pool(storage=storage, max_slots=4, inplace=inplace)
     s = pool.admit(sv.host_state(req))
     for n in schedule:
         pool.advance(n)
@@ -318,3 +318,39 @@ def test_server_cancels_queued_and_running_requests():
     assert not by[0].cancelled and by[0].steps >= 1000 and np.isfinite(by[0].stress)
     assert pool.usage()[2] == 0
     pool.close()
+
+
+
+@pytest.mark.parametrize("storage", [0, 1])
+def test_inplace_pool_matches_two_buffer_pool(storage):
+    # Members with one distribution buffer (in place): identical alone and in
+    # the mix with late joins, and bit for bit the two-buffer members.
+    pool = d3.Pool(storage=storage, max_slots=8, inplace=True)
+    s0 = pool.admit(sv.host_state(REQS[0]))
+    s1 = pool.admit(sv.host_state(REQS[1]))
+    pool.advance(100)
+    s3 = pool.admit(sv.host_state(REQS[3]))
+    pool.advance(60)
+    got = {0: state(pool, s0), 1: state(pool, s1), 3: state(pool, s3)}
+    # A two-buffer member does not join an in-place pool.
+    with pytest.raises(d3.D3Q19Error, match="EINVAL"):
+        pool.admit(sv.host_state(REQS[2]), inplace=0)
+    pool.close()
+    bits_equal(got[0], alone(REQS[0], storage, [100, 60]))
+    bits_equal(got[0], alone(REQS[0], storage, [160], inplace=True))
+    bits_equal(got[1], alone(REQS[1], storage, [160]))
+    bits_equal(got[3], alone(REQS[3], storage, [60]))
+
+
+def test_inplace_pool_evict_and_readmit():
+    pool = d3.Pool(storage=0, max_slots=4, inplace=True)
+    sa = pool.admit(sv.host_state(REQS[0]))
+    sb = pool.admit(sv.host_state(REQS[1]))
+    pool.advance(40)
+    ev = pool.evict(sa)
+    pool.advance(20)
+    sa = pool.readmit(ev)
+    pool.advance(40)
+    got = state(pool, sa)
+    pool.close()
+    bits_equal(got, alone(REQS[0], 0, [80]))
