@@ -13,7 +13,11 @@ Metric: MLUPS = interior nodes x steps / s / 1e6, summed over GPUs (each GPU
 runs an independent replica: weak scaling, no collective on the data path).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--storage fp32|fp16|bf16] [--inplace]
+                    [--storage fp32|fp16|bf16] [--two-buffers]
+
+The distributions are kept in one buffer updated in place (the AA pattern,
+d3q19_options.inplace = 1), which gives results bit-identical to the
+reference's two buffers; --two-buffers measures that layout instead.
 
 Other modes (--workload, one GPU, one JSON line each): powerlaw-128-fluid and
 couette-sphere-64 (the same line for the fluid alone and the 64^3 single
@@ -183,10 +187,10 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(workload, storage="fp32"):
+def ncu_traffic(workload, storage="fp32", inplace=False):
     """DRAM bytes per launch of the collide-stream kernel from the committed
     ncu summary (profiles/), or None."""
-    suffix = "" if storage == "fp32" else "_" + storage
+    suffix = ("" if storage == "fp32" else "_" + storage) + ("_inplace" if inplace else "")
     p = os.path.join(REPO, "profiles", f"fluid_step_kernel_{workload}{suffix}.json")
     try:
         with open(p) as fh:
@@ -354,7 +358,7 @@ def run_ours(args, rank, world, local_rank, dist):
                    "distribution_buffers": 1 if args.inplace else 2},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
-                     "traffic": None if args.inplace else ncu_traffic(args.workload, args.storage),
+                     "traffic": ncu_traffic(args.workload, args.storage, args.inplace),
                      "kernel": "fluid_step_kernel", "bytes_per_node": bytes_per_node,
                      "kernel_ms": round(fluid_avg, 5), "particle_kernel_ms": round(part_avg, 5),
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
@@ -737,11 +741,13 @@ def main():
                                                                                            "casson-precision"])
     ap.add_argument("--requests", type=int, default=128, help="served-sweep: number of requests")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--inplace", action="store_true",
-                    help="one distribution buffer updated in place (AA pattern) instead of two")
+    ap.add_argument("--two-buffers", action="store_true",
+                    help="the reference's two distribution buffers instead of one updated in place (AA pattern); "
+                         "the results are bit-identical either way")
     ap.add_argument("--storage", default="fp32", choices=sorted(STORAGE),
                     help="distribution storage: fp32 (the reference's), or 16-bit shifted")
     args = ap.parse_args()
+    args.inplace = not args.two_buffers
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     world = int(os.environ.get("WORLD_SIZE", "1"))
