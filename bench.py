@@ -488,7 +488,9 @@ def run_batch(args):
     nodes = sum((hs.cfg.ip.LatticeSize[0] - 2) * (hs.cfg.ip.LatticeSize[1] - 2) * (hs.cfg.ip.LatticeSize[2] - 2)
                 for hs in states)
     chunk = 1000
-    pool = d3.Pool(storage=1, max_slots=len(states), hbm_budget=120 << 30)
+    # Two buffers: with these small FP16 boxes they measured faster than the
+    # in-place layout (17,573 against 16,593 MLUPS), unlike the served FP32 pools.
+    pool = d3.Pool(storage=1, max_slots=len(states), hbm_budget=120 << 30, inplace=False)
     for hs in states:
         if pool.admit(hs) is None:
             raise RuntimeError("batch does not fit the pool")
@@ -546,7 +548,7 @@ def warm_served_paths(storages, alone=True):
 
     reqs = sv.make_requests(12, 0.0, 99, edges=(32, 64))
     for storage in storages:
-        pool = d3.Pool(storage=storage, max_slots=64, hbm_budget=4 << 30)
+        pool = d3.Pool(storage=storage, max_slots=64, hbm_budget=4 << 30, inplace=True)
         sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=2000).run(reqs)
         pool.close()
     if alone:
@@ -571,7 +573,7 @@ def run_served(args):
     warm_served_paths((0, 1))
     runs = {}
     for storage in (0, 1):
-        pool = d3.Pool(storage=storage, max_slots=256, hbm_budget=100 << 30)
+        pool = d3.Pool(storage=storage, max_slots=256, hbm_budget=100 << 30, inplace=args.inplace)
         runs[storage] = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=max_steps).run(reqs)
         pool.close()
     served, served16 = sv.summary(*runs[0]), sv.summary(*runs[1])
@@ -590,7 +592,8 @@ def run_served(args):
             "data": "synthetic (seeded Poisson arrivals)", "impl": "ours",
             "config": {"workload": "served-sweep", "requests": len(reqs), "arrival_rate_per_s": 50.0,
                        "edges": [32, 64], "phi": [0.0, 0.3], "models": list(sv.MODELS), "stop": "1e-4 over 500 steps",
-                       "max_steps": max_steps, "pool_storage": "fp32"},
+                       "max_steps": max_steps, "pool_storage": "fp32",
+                       "pool_layout": "in place" if args.inplace else "two buffers"},
             "served": served, "served_fp16_pool": served16, "one_at_a_time_fp32": alone,
             "speedup_solves_per_s": round(served["solves_per_s"] / alone["solves_per_s"], 2),
             "speedup_fp16_pool": round(served16["solves_per_s"] / alone["solves_per_s"], 2),
@@ -621,7 +624,7 @@ def run_served_preempt(args):
     warm_served_paths((0,), alone=False)
     out = {}
     for label, pre in (("arrival_order", None), ("preempt_2000", 2000)):
-        pool = d3.Pool(storage=0, max_slots=64, hbm_budget=budget)
+        pool = d3.Pool(storage=0, max_slots=64, hbm_budget=budget, inplace=args.inplace)
         cost = {"evict_s": 0.0, "readmit_s": 0.0, "bytes": 0, "n": 0}
         ev, re = pool.evict, pool.readmit
 

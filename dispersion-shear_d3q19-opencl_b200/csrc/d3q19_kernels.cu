@@ -124,9 +124,7 @@ struct Stored;
 // store_stream: the same value with an evict-first (streaming) store.  The
 // in-place steps write the cells the next step reads; streaming the writes
 // keeps more of them, and the rows neighbouring tiles still read, in L2.
-__device__ __forceinline__ void stcs_u16(void* p, unsigned short v) {
-  asm volatile("st.global.cs.b16 [%0], %1;" ::"l"(p), "h"(v) : "memory");
-}
+__device__ __forceinline__ void stcs_u16(void* p, unsigned short v) { __stcs(static_cast<unsigned short*>(p), v); }
 // load/store take and give f_q (the 16-bit forms through load_dev and
 // store_dev, which give and take the stored deviation f_q - w_q).
 template <>
