@@ -825,15 +825,11 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
     const R jz = f[5] - f[6] + f[9] - f[10] + f[13] - f[14] + f[15] - f[16] + f[17] - f[18];
     const R ir = RMath<R>::rcp(rho);
     const R ux = (jx + R(0.5f) * gx) * ir, uy = (jy + R(0.5f) * gy) * ir, uz = (jz + R(0.5f) * gz) * ir;
-    if (AA) {  // streamed with the populations (see Stored::store_stream)
-      __stcs(a.u + i, (float)ux);
-      __stcs(a.u + i + NC, (float)uy);
-      __stcs(a.u + i + 2 * NC, (float)uz);
-    } else {
-      a.u[i] = (float)ux;
-      a.u[i + NC] = (float)uy;
-      a.u[i + 2 * NC] = (float)uz;
-    }
+    // Plain stores (also in place): the particle pass reads u right after,
+    // from L2.
+    a.u[i] = (float)ux;
+    a.u[i + NC] = (float)uy;
+    a.u[i + 2 * NC] = (float)uz;
     // A non-finite population makes rho non-finite; a vanishing or negative
     // density is flagged too.
     if (!(rho > R(0) && rho < R(1e30f))) atomicOr(a.err, ERR_NONFINITE);
