@@ -5,7 +5,9 @@ ids read from the tile lists, interpolation stencils, zone and sphere ids of
 the contact search) and report D3Q19_EBOUNDS instead of touching memory
 outside an array.  Here it runs in a child process (the build is chosen when
 the library is first loaded) on cases that exercise periodic wrap, wrapping
-sphere stencils, tile-edge markers, contacts and the batched pool.  It must
+sphere stencils, tile-edge markers, contacts and the batched pool, each with
+two distribution buffers and in place (the in-place odd step pulls from
+upwind and pushes downwind, so its indices are checked too).  It must
 report nothing, and its results must be bit-identical to the default
 build's, since the checks change no arithmetic.
 """
@@ -21,6 +23,7 @@ pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASE_NAMES = ["sphere_wrap", "wrap_tile_edge", "contacts", "power_law_sphere", "periodic_force"]
+INPLACE_NAMES = ["sphere_wrap", "wrap_tile_edge", "contacts", "couette", "xwall_tangential"]
 
 
 def compute(out_path):
@@ -33,27 +36,31 @@ def compute(out_path):
     from d3q19_b200 import serving as sv
 
     res = {}
-    for name in CASE_NAMES:
+    runs = [(n, 0) for n in CASE_NAMES] + [(n, 1) for n in INPLACE_NAMES]
+    for name, inplace in runs:
         g = load_golden(name)
-        sim, ip, fp = sim_from_golden(g, CASES[name])
-        sim.run(1, 3 * CASES[name]["iterations"])
+        sim, ip, fp = sim_from_golden(g, CASES[name], inplace=inplace)
+        sim.run(1, 3 * CASES[name]["iterations"] + inplace)  # in place: end on an odd step
         sim.synchronize()
-        res[f"{name}/u"] = sim.read_u()
+        key = f"{name}/ip{inplace}"
+        res[f"{key}/u"] = sim.read_u()
+        res[f"{key}/f"] = sim.read_f()
         if sim.np > 0:
-            res[f"{name}/kin"] = sim.read_parkin()
-            res[f"{name}/pff"] = sim.read_parfluidforce()
-            res[f"{name}/gpf"] = sim.read_spread_force()
+            res[f"{key}/kin"] = sim.read_parkin()
+            res[f"{key}/pff"] = sim.read_parfluidforce()
+            res[f"{key}/gpf"] = sim.read_spread_force()
         sim.close()
-    pool = d3.Pool(storage=1, max_slots=4)
     reqs = [sv.ShearRequest(rid=0, edge=(34, 34, 34), phi=0.25, model="power_law", wall_speed=0.03, seed=5),
             sv.ShearRequest(rid=1, edge=(32, 40, 36), phi=0.2, model="casson", wall_speed=0.02, seed=6)]
-    slots = [pool.admit(sv.host_state(r)) for r in reqs]
-    pool.advance(100)
-    st, _, _, code = pool.mean_stress_all(4)
-    for k, s in enumerate(slots):
-        assert code[s] == 0, (k, d3.STATUS[int(code[s])])
-        res[f"pool{k}/u"] = pool.member(s).read_u()
-    pool.close()
+    for inplace in (False, True):
+        pool = d3.Pool(storage=1, max_slots=4, inplace=inplace)
+        slots = [pool.admit(sv.host_state(r)) for r in reqs]
+        pool.advance(110)
+        st, _, _, code = pool.mean_stress_all(4)
+        for k, s in enumerate(slots):
+            assert code[s] == 0, (k, inplace, d3.STATUS[int(code[s])])
+            res[f"pool{k}/ip{int(inplace)}/u"] = pool.member(s).read_u()
+        pool.close()
     np.savez(out_path, **res)
 
 
