@@ -57,6 +57,18 @@ __device__ __forceinline__ bool out_of_bounds(long long idx, long long n, unsign
   return false;
 }
 
+// Programmatic dependent launch of the step's collide-stream and particle
+// passes (each launched with programmatic stream serialization): a pass's
+// blocks may be scheduled while the pass before it in the stream is still
+// running, so its launch and block set-up overlap that pass's last wave.
+// pdl_wait() returns once every grid the pass depends on has completed and
+// its writes are visible (at once when the launch had no such dependency);
+// every read or write of another pass's data comes after it.  pdl_trigger()
+// lets the next pass's blocks be scheduled; it is issued only after the wait,
+// so a pass never starts before the pass two back has completed.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // D3Q19 velocities in the reference's order (D3Q19-OpenCL.c:9-13), as
 // compile-time expressions of q so fully unrolled loops fold them.
 #define CXQ(q) (((q) == 1 || (q) == 7 || (q) == 8 || (q) == 9 || (q) == 10) ? 1 : \
@@ -877,6 +889,10 @@ __global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4   ? (AA ? FLUID
                                                                    : FLUID_MIN_BLOCKS)
     fluid_step_kernel(const FluidArgs a, const int first) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  // Everything here reads or writes data of the passes before it: the tile
+  // lists, the distributions, and u, which the previous particle pass reads.
+  pdl_wait();
+  pdl_trigger();
   fluid_tile<COLL, VISC, BC, ST, AA>(a, first, blockIdx.x, blockIdx.y, blockIdx.z,
                                      *reinterpret_cast<SpreadSmem*>(smem_raw));
 }
@@ -1190,6 +1206,10 @@ __device__ __forceinline__ void particle_group(const ParticleArgs& a, const int 
     const int wg = grp - p * nfa;  // work-group of the sphere
     // The rigid-body update of the sphere, once per block and shared.
     const float4 r0 = l < L ? a.sphere[wg * L + l] : make_float4(0.f, 0.f, 0.f, 0.f);
+    // The marker template above is constant; the rigid-body update reads the
+    // contact forces of the side stream's pass, so it waits too.
+    pdl_wait();
+    pdl_trigger();
     if (l == 0) {
       const Kin kn = rigid_update(a, p);
       s_kin = kn;
@@ -1723,15 +1743,35 @@ __global__ void load_f_kernel(const ST* __restrict__ in, float* __restrict__ out
 
 // ---------------------------------------------------------------------------
 // Launchers.
+
+// A launch whose blocks may be scheduled before the previous kernel in the
+// stream has completed (programmatic dependent launch); the kernel orders its
+// accesses with pdl_wait().
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_overlapped(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                     Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <int COLL, int VISC, int BC, typename ST>
 static cudaError_t launch_fluid_t(const FluidArgs& a, bool first, cudaStream_t s) {
   dim3 block(TILE_X, TILE_Y, 2);
   dim3 grid(a.g.ntx, a.g.nty, a.g.ntz);
   const size_t smem = fluid_smem_bytes(a.has_ibm != 0);
-  if (a.inplace == 1) fluid_step_kernel<COLL, VISC, BC, ST, 1><<<grid, block, smem, s>>>(a, first ? 1 : 0);
-  else if (a.inplace == 2) fluid_step_kernel<COLL, VISC, BC, ST, 2><<<grid, block, smem, s>>>(a, first ? 1 : 0);
-  else fluid_step_kernel<COLL, VISC, BC, ST, 0><<<grid, block, smem, s>>>(a, first ? 1 : 0);
-  return cudaGetLastError();
+  const int fi = first ? 1 : 0;
+  if (a.inplace == 1) return launch_overlapped(fluid_step_kernel<COLL, VISC, BC, ST, 1>, grid, block, smem, s, a, fi);
+  if (a.inplace == 2) return launch_overlapped(fluid_step_kernel<COLL, VISC, BC, ST, 2>, grid, block, smem, s, a, fi);
+  return launch_overlapped(fluid_step_kernel<COLL, VISC, BC, ST, 0>, grid, block, smem, s, a, fi);
 }
 
 template <int COLL, int BC, typename ST>
@@ -1804,8 +1844,7 @@ cudaError_t launch_particles(const ParticleArgs& a, cudaStream_t s) {
     return cudaGetLastError();
   }
   const size_t smem = sizeof(float4) * 2 * threads;
-  particle_step_kernel<<<ngroups, threads, smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_overlapped(particle_step_kernel, dim3(ngroups), dim3(threads), smem, s, a);
 }
 
 cudaError_t launch_contacts(const ParticleArgs& a, cudaStream_t s) {
