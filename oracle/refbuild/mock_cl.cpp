@@ -27,6 +27,9 @@
 // Environment:
 //   MOCKCL_KERNEL_WG_SIZE  value reported for CL_KERNEL_WORK_GROUP_SIZE (256)
 //   MOCKCL_SERIAL          1 = run every kernel serially, groups in order
+//   MOCKCL_SERIAL_FIBERS   1 = run the kernel with barrier() (the IBM spread,
+//                          whose slot updates race between concurrent groups)
+//                          in group order, the other kernels in parallel
 //   MOCKCL_THREADS         host threads (default: all)
 //   MOCKCL_DUMP_DIR        dump every buffer to <dir>/buf_<creation#>.bin when
 //                          the host releases it (sim_main.c:510-512)
@@ -387,7 +390,7 @@ extern "C" cl_int clEnqueueNDRangeKernel(cl_command_queue, cl_kernel k, cl_uint 
   int mode = k->def.mode;
   if (mode == MODE_FIBERS) {
     size_t ng = L.ngrp[0] * L.ngrp[1] * L.ngrp[2];
-    if (serial) {
+    if (serial || env_int("MOCKCL_SERIAL_FIBERS", 0) != 0) {
       fiber_group fg;
       for (size_t g = 0; g < ng; g++)
         run_group_fibers(fg, L, g % L.ngrp[0], (g / L.ngrp[0]) % L.ngrp[1], g / (L.ngrp[0] * L.ngrp[1]));

@@ -50,3 +50,7 @@ def sim_from_golden(g, case, **over):
         sim.write_zones(g["init_zoneNeighDat"], g["init_parsZone"], zm, g["init_numParInZone"], tm,
                         g["init_numParInThread"])
     return sim, ip, fp
+
+
+# The reference's compute_shear_stress quantities from a velocity field.
+from fullsize_cases import shear_quantities as reference_shear  # noqa: E402,F401

@@ -13,7 +13,7 @@ import pytest
 
 from conftest import load_golden
 from cases import CASES, is_variable
-from gpu_helpers import REL_TOL, rel_l2, sim_from_golden
+from gpu_helpers import REL_TOL, reference_shear, rel_l2, sim_from_golden
 from test_gpu_parity import bound
 
 pytestmark = pytest.mark.gpu
@@ -52,26 +52,6 @@ def plane_sums(u, tau, ip, fp, variable):
         out[z] = [U[0, z, ys, 1:-1].sum(), U[1, z, ys, 1:-1].sum(), U[2, z, ys, 1:-1].sum(), gxz.sum(),
                   (nu * gxz).sum()]
     return out
-
-
-def reference_shear(u, ip, fp):
-    """The reference's compute_shear_stress quantities from a velocity field."""
-    Nx, Ny, Nz = ip.LatticeSize
-    U = u.astype(np.float64).reshape(3, Nz, Ny, Nx)
-    nxy = (Nx - 2) * (Ny - 2)
-    mean = np.array([[U[d, z, 1:-1, 1:-1].sum() / nxy for d in range(3)] for z in range(Nz)])
-    dz, zA, zB = 4, 6, Nz - 3
-    s = 0.0
-    if 1 <= zA <= Nz - 2:
-        s += (U[0, zA, 1:-1, 1:-1] - U[0, zA - dz, 1:-1, 1:-1]).sum() / dz
-    if zB != zA and 1 <= zB <= Nz - 2 and zB - dz >= 0:
-        s += (U[0, zB, 1:-1, 1:-1] - U[0, zB - dz, 1:-1, 1:-1]).sum() / dz
-    wall = s / (2.0 * nxy)
-    ib = int(fp.ParticleZBuffer + 1e-8) + int(fp.ParticleDiam / 2)
-    zbL, zbU = 1 + ib, Nz - 2 - ib
-    ok = 0 <= zbL < Nz and 0 <= zbU < Nz and zbU != zbL
-    region = (mean[zbU, 0] - mean[zbL, 0]) / (zbU - zbL) if ok else 0.0
-    return mean, wall, region
 
 
 @pytest.mark.parametrize("name", SHEAR_CASES)
