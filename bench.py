@@ -200,7 +200,10 @@ def ncu_traffic(workload, storage="fp32", inplace=False):
         return None
 
 
-def setup(workload, device, storage="fp32", inplace=False):
+FLUID_KERNELS = {"tile": 0, "tma": 1}
+
+
+def setup(workload, device, storage="fp32", inplace=False, fluid_kernel="tile"):
     import numpy as np  # noqa: F401
 
     import d3q19_b200 as d3
@@ -210,7 +213,9 @@ def setup(workload, device, storage="fp32", inplace=False):
     hs.options.device = device
     hs.options.storage = STORAGE[storage][0]
     hs.options.inplace = int(inplace)
-    sim = d3.Simulation.from_host_state(hs, device=device, storage=STORAGE[storage][0], inplace=int(inplace))
+    hs.options.fluid_kernel = FLUID_KERNELS[fluid_kernel]
+    sim = d3.Simulation.from_host_state(hs, device=device, storage=STORAGE[storage][0], inplace=int(inplace),
+                                        fluid_kernel=FLUID_KERNELS[fluid_kernel])
     return d3, hs, sim
 
 
@@ -262,7 +267,8 @@ def run_ours(args, rank, world, local_rank, dist):
     import torch
 
     torch.cuda.set_device(local_rank)
-    d3, hs, sim = setup(args.workload, local_rank, args.storage, args.inplace)
+    d3, hs, sim = setup(args.workload, local_rank, args.storage, args.inplace, args.fluid_kernel)
+    kernel_name = {"tma": "fluid_tma_kernel", "tile": "fluid_step_kernel"}.get(sim.fluid_kernel, sim.fluid_kernel)
     bytes_per_node = STORAGE[args.storage][1]
     ip = hs.cfg.ip
     interior = (ip.LatticeSize[0] - 2) * (ip.LatticeSize[1] - 2) * (ip.LatticeSize[2] - 2)
@@ -359,7 +365,7 @@ def run_ours(args, rank, world, local_rank, dist):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": ncu_traffic(args.workload, args.storage, args.inplace),
-                     "kernel": "fluid_step_kernel", "bytes_per_node": bytes_per_node,
+                     "kernel": kernel_name, "bytes_per_node": bytes_per_node,
                      "kernel_ms": round(fluid_avg, 5), "particle_kernel_ms": round(part_avg, 5),
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                      "fallback 6.65 TB/s",
@@ -744,6 +750,9 @@ def main():
                                                                                            "casson-precision"])
     ap.add_argument("--requests", type=int, default=128, help="served-sweep: number of requests")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fluid-kernel", default="tile", choices=sorted(FLUID_KERNELS),
+                    help="collide-stream kernel: tile (the per-tile kernel) or tma (the TMA-pipelined kernel "
+                         "where the lattice allows it)")
     ap.add_argument("--two-buffers", action="store_true",
                     help="the reference's two distribution buffers instead of one updated in place (AA pattern); "
                          "the results are bit-identical either way")

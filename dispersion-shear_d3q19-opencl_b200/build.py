@@ -24,12 +24,13 @@ MAIN = os.path.join(BIN, "d3q19_b200")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SRC = [os.path.join(PKG, "csrc", f) for f in ("d3q19_kernels.cu", "d3q19_api.cu", "d3q19_exact.cu")]
+CU_SRC = [os.path.join(PKG, "csrc", f) for f in ("d3q19_kernels.cu", "d3q19_api.cu", "d3q19_exact.cu", "d3q19_tma.cu")]
 # Translation units compiled without floating-point contraction: the
 # reference-exact arithmetic.
 NO_CONTRACT = {"d3q19_exact.cu"}
 OBJ = os.path.join(PKG, "_build")
-CU_HDR = [os.path.join(PKG, "csrc", "d3q19_internal.h"), os.path.join(REPO, "include", "d3q19_b200.h")]
+CU_HDR = [os.path.join(PKG, "csrc", "d3q19_internal.h"), os.path.join(PKG, "csrc", "d3q19_device.cuh"),
+          os.path.join(REPO, "include", "d3q19_b200.h")]
 HOST_SRC = [os.path.join(PKG, "host", "d3q19_host.c")]
 HOST_HDR = [os.path.join(PKG, "host", "d3q19_host.h"), os.path.join(REPO, "include", "d3q19_b200.h")]
 MAIN_SRC = [os.path.join(PKG, "host", "d3q19_main.c")]

@@ -83,6 +83,10 @@ struct d3q19_ctx {
   int* revList = nullptr;
   int* zoneOf = nullptr;
   int nzones = 0;
+  // The TMA-pipelined collide-stream kernel (d3q19_tma.cu) and its tensor
+  // maps, when the context allows it (fluid_kernel 0).
+  TmaMaps tma;
+  bool use_tma = false;
   unsigned* err = nullptr;
   unsigned long long* clamps = nullptr;
   double* pstats = nullptr;  // per-plane FP64 sums [5 * Nz]
@@ -366,6 +370,8 @@ static int create_ctx(const int_param_struct* ip, const flp_param_struct* fp, co
     cudaMemsetAsync(c->fmax, 0, sizeof(unsigned) * 2, c->stream);
     cudaMemsetAsync(c->mrec, 0, sizeof(float4) * 2 * M, c->stream);
   }
+  if (o.fluid_kernel == 1 && o.arithmetic == 0 && o.collision == 0 && tma_supported(g, o.storage))
+    c->use_tma = tma_make_maps(&c->tma, c->f, g, o.storage);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
     snprintf(g_create_error, sizeof(g_create_error), "initialisation failed");
     d3q19_destroy(c);
@@ -373,6 +379,11 @@ static int create_ctx(const int_param_struct* ip, const flp_param_struct* fp, co
   }
   *out = c;
   return 0;
+}
+
+extern "C" int d3q19_fluid_kernel(const d3q19_ctx* c) {
+  if (!c) return D3Q19_EINVAL;
+  return c->opt.arithmetic == 1 ? 2 : (c->use_tma ? 1 : 0);
 }
 
 extern "C" int d3q19_write_lattice(d3q19_ctx* c, const float* f, const float* u, const float* tau_lb) {
@@ -633,6 +644,15 @@ static ZoneArgs zone_args(const d3q19_ctx* c, int pnew) {
   return za;
 }
 
+// The collide-stream pass of step t on the context's stream.
+static cudaError_t fluid_pass(d3q19_ctx* c, const FluidArgs& fa) {
+  const bool first = c->f_state == 1;
+  if (c->opt.arithmetic == 1)
+    return launch_fluid_exact(fa, first, c->opt.variable_viscosity != 0, c->ip.MaxSurfPointsPerNode, c->stream);
+  if (c->use_tma) return launch_fluid_tma(c->tma, c->cur, fa, first, c->opt.storage, c->stream);
+  return launch_fluid(fa, first, c->opt.variable_viscosity != 0, c->opt.collision, c->opt.storage, c->stream);
+}
+
 static int enqueue_step(d3q19_ctx* c, int t) {
   const FluidArgs fa = fluid_args(c, t, c->cur);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -641,12 +661,7 @@ static int enqueue_step(d3q19_ctx* c, int t) {
     CUDA_TRY(c, cudaEventCreate(&e1));
     CUDA_TRY(c, cudaEventRecord(e0, c->stream));
   }
-  if (c->opt.arithmetic == 1)
-    CUDA_TRY(c, launch_fluid_exact(fa, c->f_state == 1, c->opt.variable_viscosity != 0, c->ip.MaxSurfPointsPerNode,
-                                   c->stream));
-  else
-    CUDA_TRY(c, launch_fluid(fa, c->f_state == 1, c->opt.variable_viscosity != 0, c->opt.collision, c->opt.storage,
-                             c->stream));
+  CUDA_TRY(c, fluid_pass(c, fa));
   if (c->profiling) {
     CUDA_TRY(c, cudaEventRecord(e1, c->stream));
     c->ev_fluid.emplace_back(e0, e1);
@@ -693,12 +708,7 @@ extern "C" int d3q19_k_collide_stream(d3q19_ctx* c, int t) {
   if (c->side_pending) CUDA_TRY(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
   c->side_pending = false;
   const FluidArgs fa = fluid_args(c, t, c->cur);
-  if (c->opt.arithmetic == 1)
-    CUDA_TRY(c, launch_fluid_exact(fa, c->f_state == 1, c->opt.variable_viscosity != 0, c->ip.MaxSurfPointsPerNode,
-                                   c->stream));
-  else
-    CUDA_TRY(c, launch_fluid(fa, c->f_state == 1, c->opt.variable_viscosity != 0, c->opt.collision, c->opt.storage,
-                             c->stream));
+  CUDA_TRY(c, fluid_pass(c, fa));
   c->cur = 1 - c->cur;
   c->f_state = 2;
   c->last_t = t;
@@ -820,6 +830,8 @@ static int device_errors(d3q19_ctx* c) {
   if (c->sticky & (ERR_NONFINITE | ERR_FIXED_RANGE))
     return fail(c, D3Q19_ENUMERIC, "non-finite or out-of-range density, velocity or marker position on the device");
   if (c->sticky & ERR_ZONE_RANGE) return fail(c, D3Q19_ENUMERIC, "sphere position outside the zone grid");
+  if (c->sticky & ERR_TIMEOUT)
+    return fail(c, D3Q19_ETIMEDOUT, "a TMA load of the collide-stream pass did not complete within its limit");
   return 0;
 }
 
@@ -1224,7 +1236,7 @@ const char* ckpt_tables_invalid(d3q19_ctx* c, const char* data) {
   if (np == 0) return nullptr;
   const long long M = np * c->ppar.P, Z = c->nzones, cap = c->tile_cap;
   const int *tile_count = nullptr, *tile_list = nullptr, *znd = nullptr, *members = nullptr, *nin = nullptr,
-            *rstart = nullptr, *rlist = nullptr;
+            *rstart = nullptr, *rlist = nullptr, *pzone = nullptr, *zoneof = nullptr;
   size_t off = 0;
   for (const auto& b : ckpt_blocks(c)) {
     const int* q = reinterpret_cast<const int*>(data + off);
@@ -1236,6 +1248,8 @@ const char* ckpt_tables_invalid(d3q19_ctx* c, const char* data) {
     else if (n == "numParInZone") nin = q;
     else if (n == "revStart") rstart = q;
     else if (n == "revList") rlist = q;
+    else if (n == "parsZone") pzone = q;
+    else if (n == "zoneOf") zoneof = q;
     off += b.bytes;
   }
   for (long long T = 0; T < c->ntiles; T++) {
@@ -1246,9 +1260,15 @@ const char* ckpt_tables_invalid(d3q19_ctx* c, const char* data) {
   }
   for (long long z = 0; z < Z; z++) {
     if (znd[28 * z] < 0 || znd[28 * z] > 27) return "zone neighbour count";
+    for (long long t = 1; t <= znd[28 * z]; t++)
+      if (znd[28 * z + t] < 0 || znd[28 * z + t] >= Z) return "zone neighbour";
     if (nin[z] < 0 || nin[z] > np) return "zone member count";
     for (long long j = 0; j < nin[z]; j++)
       if (members[z * np + j] < 0 || members[z * np + j] >= np) return "zone member";
+  }
+  for (long long p = 0; p < np; p++) {
+    if (pzone[p] < 0 || pzone[p] >= Z) return "sphere zone";
+    if (zoneof[p] < 0 || zoneof[p] >= Z) return "sphere zone";
   }
   if (rstart[0] != 0 || rstart[Z] > 27 * Z) return "reverse zone table";
   for (long long z = 0; z < Z; z++)
@@ -1318,6 +1338,9 @@ extern "C" int d3q19_restore(d3q19_ctx* c, const void* buf, size_t bytes) {
       h.NC != c->g.NC || h.ntiles != c->ntiles || h.np != c->ppar.np || h.nfa != c->ppar.nfa || h.P != c->ppar.P ||
       h.cap != c->tile_cap || h.nzones != c->nzones || h.inplace != c->opt.inplace)
     return fail(c, D3Q19_EINVAL, "checkpoint of a context with other parameters");
+  if ((c->opt.inplace && h.phase != 0 && h.phase != 1) || (h.f_state != 1 && h.f_state != 2) || h.last_t < 0 ||
+      (h.f_state == 1 && c->opt.inplace && h.phase != 0))
+    return fail(c, D3Q19_EINVAL, "checkpoint damaged: header state out of range");
   size_t need = 0;
   d3q19_checkpoint_bytes(c, &need);
   if (bytes < need) return fail(c, D3Q19_EINVAL, "checkpoint truncated (%zu of %zu bytes)", bytes, need);
@@ -1341,6 +1364,14 @@ extern "C" int d3q19_restore(d3q19_ctx* c, const void* buf, size_t bytes) {
   c->f_state = h.f_state;
   c->last_t = h.last_t;
   c->have_particles = c->have_zones = true;
+  // The TMA kernel's pulls read periodic neighbours' values from the
+  // buffer-layer copies the step before it wrote; a restored buffer gets them
+  // from its periodic images.
+  if (c->use_tma && c->f_state == 2 && (!c->opt.inplace || c->cur == 1)) {
+    FluidArgs fa = fluid_args(c, c->last_t, c->cur);
+    CUDA_TRY(c, launch_fill_ghosts(fa, c->opt.storage, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
   return 0;
 }
 
@@ -1516,6 +1547,10 @@ static int pool_place(d3q19_pool* p, const int_param_struct* ip, const d3q19_opt
       o.tangential_vel_bc[0] || o.tangential_vel_bc[1] || o.tangential_vel_bc[2])
     return pfail(p, D3Q19_EINVAL, "the pool runs shear cells: periodic x and y, velocity walls on z");
   if (o.rebuild_freq <= 0) o.rebuild_freq = 10;
+  // Members are advanced by the batched per-tile kernels, which fold the
+  // periodic wrap into their gathers; their solo warm-up steps use the same
+  // kernel family.
+  o.fluid_kernel = 0;
   if (ip->NumParticles > 0 && o.rebuild_freq != p->rebuild)
     return pfail(p, D3Q19_EINVAL, "rebuild_freq %d differs from the pool's %d", o.rebuild_freq, p->rebuild);
   if (ip->NumParticles > 0 && ip->PointsPerWorkGroup > 256)

@@ -34,6 +34,7 @@ constexpr unsigned ERR_NONFINITE = 2u;
 constexpr unsigned ERR_ZONE_RANGE = 4u;
 constexpr unsigned ERR_FIXED_RANGE = 8u;
 constexpr unsigned ERR_BOUNDS = 16u;  // an index check of the bounds-checked build failed (access skipped)
+constexpr unsigned ERR_TIMEOUT = 32u;  // a bounded device wait (a TMA load of the collide-stream pass) ran out
 
 struct Geom {
   int Nx, Ny, Nz;
@@ -155,6 +156,22 @@ constexpr int STORE_F32 = 0, STORE_F16 = 1, STORE_BF16 = 2, STORE_F64 = 3;
 inline int storage_bytes(int storage) { return storage == STORE_F32 ? 4 : (storage == STORE_F64 ? 8 : 2); }
 
 cudaError_t launch_fluid(const FluidArgs& a, bool first, bool variable, int collision, int storage, cudaStream_t s);
+// The TMA-pipelined collide-stream pass (d3q19_tma.cu): tensor maps of the
+// distribution buffers (boxes of the tile width, and x-widened boxes for the
+// pulls), made once per context.  tma_supported: the context's geometry and
+// storage allow it (periodic x/y with z walls, FP32 / 16-bit storage,
+// 16-byte aligned x rows).  buf: the buffer the step reads.
+struct TmaMaps {
+  alignas(64) unsigned char f[2][2][128];
+  int ready = 0;
+};
+bool tma_supported(const Geom& g, int storage);
+bool tma_make_maps(TmaMaps* m, void* const f[2], const Geom& g, int storage);
+cudaError_t launch_fluid_tma(const TmaMaps& m, int buf, const FluidArgs& a, bool first, int storage, cudaStream_t s);
+// Copies every population of the periodic x/y buffer-layer nodes of a.fin
+// from their periodic images (the copies the TMA kernel's pulls read), for a
+// buffer the TMA kernel did not write itself (a restored checkpoint).
+cudaError_t launch_fill_ghosts(const FluidArgs& a, int storage, cudaStream_t s);
 cudaError_t launch_materialize_f(const FluidArgs& a, int storage, float* out, cudaStream_t s);
 // Conversions between float distributions and the stored form (n values,
 // row q of each N_C-long row block shifted by w_q).

@@ -23,7 +23,7 @@ HOST_LIB = os.path.join(LIBDIR, "libd3q19_host.so")
 # Largest lattice (N_C nodes) d3q19_read_spread_force_static accepts.
 STATIC_SPREAD_MAX_CELLS = 262144
 STATUS = {0: "OK", -1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ENODEV", -5: "EOVERFLOW", -6: "ENUMERIC",
-          -7: "ESTATE", -8: "EBUSY", -9: "EBOUNDS"}
+          -7: "ESTATE", -8: "EBUSY", -9: "EBOUNDS", -10: "ETIMEDOUT"}
 EBUSY = -8
 
 _INT_FIELDS = [
@@ -56,7 +56,8 @@ class Options(C.Structure):
                 ("particle_precision", C.c_int), ("fixed_particles", C.c_int), ("num_par_threads", C.c_int),
                 ("rebuild_freq", C.c_int), ("tangential_vel_bc", C.c_int * 3), ("tau_max", C.c_float),
                 ("tau_min", C.c_float), ("casson_reg", C.c_float), ("device", C.c_int),
-                ("ibm_tile_capacity", C.c_int), ("arithmetic", C.c_int), ("inplace", C.c_int)]
+                ("ibm_tile_capacity", C.c_int), ("arithmetic", C.c_int), ("inplace", C.c_int),
+                ("fluid_kernel", C.c_int)]
 
 
 class DeviceInfo(C.Structure):
@@ -309,6 +310,13 @@ class Simulation:
     def _check(self, rc, what):
         if rc:
             raise D3Q19Error(f"{what}: {STATUS.get(rc, rc)}: {self.lib.d3q19_last_error(self.h).decode()}")
+
+    @property
+    def fluid_kernel(self):
+        """Collide-stream kernel of the context: 'tile' (fluid_step_kernel),
+        'tma' (the TMA-pipelined fluid_tma_kernel) or 'reference-order'."""
+        k = self.lib.d3q19_fluid_kernel(self.h)
+        return {0: "tile", 1: "tma", 2: "reference-order"}[k]
 
     def write_lattice(self, f, u, tau=None):
         f = np.ascontiguousarray(f, np.float32)

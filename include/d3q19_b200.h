@@ -76,8 +76,10 @@ enum d3q19_status {
   D3Q19_ENUMERIC = -6,  /* non-finite density or velocity detected on the device */
   D3Q19_ESTATE = -7,    /* call out of order (e.g. step before the lattice is written) */
   D3Q19_EBUSY = -8,     /* the pool has no free slot or HBM budget for the request right now */
-  D3Q19_EBOUNDS = -9    /* library built with D3Q19_BOUNDS_CHECK: a device index fell outside its array (the
+  D3Q19_EBOUNDS = -9,   /* library built with D3Q19_BOUNDS_CHECK: a device index fell outside its array (the
                            access was skipped); no counterpart in the reference */
+  D3Q19_ETIMEDOUT = -10 /* a bounded device wait ran out (a TMA load of the collide-stream pass did not complete
+                           within its limit); no counterpart in the reference */
 };
 
 /* Options with no counterpart in the reference's parameter structs.  A
@@ -140,6 +142,16 @@ typedef struct {
    * bit for bit.  Not with arithmetic 1.  The members of a lattice pool share
    * one layout.  No counterpart in the reference. */
   int inplace;
+  /* Collide-stream kernel.  0: the per-tile kernel (fluid_step_kernel).
+   * 1: the TMA-pipelined persistent kernel (fluid_tma_kernel) where the
+   * context allows it (periodic x and y with walls on z, the reference's MRT,
+   * arithmetic 0, FP32 or 16-bit storage, x extent a multiple of 4 (FP32) or
+   * 8 (16-bit) nodes), else the per-tile kernel.  The results are the same
+   * bit for bit.  On B200 the TMA kernel is the slower of the two for this
+   * step (0.0995 against 0.0743 ms per 128^3 fluid step): the step is bound
+   * by instruction issue, which staging the loads does not reduce.  No
+   * counterpart in the reference. */
+  int fluid_kernel;
 } d3q19_options;
 
 typedef struct {
@@ -164,6 +176,12 @@ int d3q19_get_device_info(int device, d3q19_device_info* out);
  * D3Q19-OpenCL.c:465-556).  Copies both parameter blocks. */
 int d3q19_create(const int_param_struct* ip, const flp_param_struct* fp, const d3q19_options* opt,
                  d3q19_ctx** out);
+
+/* Which collide-stream kernel the context runs: 0 the per-tile kernel
+ * (fluid_step_kernel), 1 the TMA-pipelined kernel (fluid_tma_kernel), 2 the
+ * reference-order kernel (arithmetic 1); negative on a null context.  No
+ * counterpart in the reference. */
+int d3q19_fluid_kernel(const d3q19_ctx* ctx);
 
 /* Replaces clEnqueueWriteBuffer of fA/fB/u/tau_lb (sim_main.c:193-198).
  * f is the state the next step reads (both reference buffers start equal);
