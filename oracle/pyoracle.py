@@ -201,3 +201,37 @@ def ref_arrays(bufs: dict) -> dict:
         else:
             out[k] = np.frombuffer(b, dtype=np.float32).copy()
     return out
+
+
+def srt_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "srt_driver"))
+
+
+def run_srt(int_bytes: bytes, flp_bytes: bytes, f, g, strMap, nsteps: int, timeout: float = 600.0, fma=False):
+    """The reference's BGK kernel collideSRT_newtonian_stream_D3Q19 with its
+    periodic and velocity boundary kernels, nsteps steps in the host's order
+    (oracle/refbuild/srt_driver.c), from distributions f (19*N_C), body-force
+    field g (3*N_C) and the periodic node list strMap.  Returns (f, u) after
+    the last step (post-boundary f).  fma: the kernels compiled with fused
+    multiply-add contraction (srt_driver_fma)."""
+    ip = IntParams.from_buffer_copy(int_bytes)
+    nc = ip.LatticeSize[0] * ip.LatticeSize[1] * ip.LatticeSize[2]
+    strMap = np.ascontiguousarray(strMap, np.int32)
+    with tempfile.TemporaryDirectory(prefix="d3q19srt_") as wd:
+        src, dst = os.path.join(wd, "in.bin"), os.path.join(wd, "out.bin")
+        with open(src, "wb") as fh:
+            fh.write(int_bytes)
+            fh.write(flp_bytes)
+            fh.write(np.array([nsteps, strMap.size // 2], np.int32).tobytes())
+            fh.write(np.ascontiguousarray(f, np.float32).tobytes())
+            fh.write(np.ascontiguousarray(g, np.float32).tobytes())
+            fh.write(strMap.tobytes())
+        shutil.copy(os.path.join(REF_DIR, "run_data", "GPU_program.cl"), os.path.join(wd, "GPU_program.cl"))
+        env = dict(os.environ, MOCKCL_QUIET="1")
+        exe = os.path.join(REF_DIR, "srt_driver_fma" if fma else "srt_driver")
+        p = subprocess.run([exe, src, dst], cwd=wd, env=env, capture_output=True,
+                           text=True, timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError(f"srt_driver failed ({p.returncode}): {p.stderr[-2000:]}")
+        out = np.fromfile(dst, np.float32)
+    return out[: 19 * nc].copy(), out[19 * nc:].copy()

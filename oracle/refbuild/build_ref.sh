@@ -23,11 +23,15 @@
 #      partitions) into oracle/_ref/run_data/ so the binaries can run where
 #      the reference tree is absent.
 #
-# Usage: oracle/refbuild/build_ref.sh [reference_dir]   (default /root/reference)
+# Usage: oracle/refbuild/build_ref.sh <reference_dir>   (or D3Q19_REFERENCE=<reference_dir>)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 REPO="$(cd "$HERE/../.." && pwd)"
-REF="${1:-${D3Q19_REFERENCE:-/root/reference}}"
+REF="${1:-${D3Q19_REFERENCE:-}}"
+if [ -z "$REF" ]; then
+  echo "usage: build_ref.sh <reference_dir> (or set D3Q19_REFERENCE)" >&2
+  exit 2
+fi
 OUT="$REPO/oracle/_ref"
 
 if [ ! -f "$REF/GPU_program.cl" ]; then
@@ -62,6 +66,20 @@ for v in const var; do
     -lm -o "$OUT/ref_${v}"
 done
 
+# The BGK driver: the reference's collideSRT_newtonian_stream_D3Q19 with its
+# boundary kernels, in the host's per-step order (srt_driver.c).
+gcc $CFLAGS -I"$HERE" -I"$REF" -c "$HERE/srt_driver.c" -o "$OUT/obj/srt_driver.o"
+g++ -fopenmp "$OUT/obj/srt_driver.o" "$OUT/obj/mock_cl.o" "$OUT/obj/kernels_cpu.o" "$OUT/obj/kernels_gpu_const.o" \
+  -lm -o "$OUT/srt_driver"
+# The same kernels compiled with fused multiply-add contraction (what an
+# OpenCL GPU compiler does by default): the reference's own rounding spread.
+if grep -q -m1 ' fma ' /proc/cpuinfo; then
+  g++ ${CXXFLAGS/-ffp-contract=off/-ffp-contract=fast} -mfma -I"$HERE" -I"$OUT" \
+    -DGPU_PROGRAM_SOURCE='"gen/GPU_program_const.cl"' -c "$HERE/kernels_gpu.cpp" -o "$OUT/obj/kernels_gpu_const_fma.o"
+  g++ -fopenmp "$OUT/obj/srt_driver.o" "$OUT/obj/mock_cl.o" "$OUT/obj/kernels_cpu.o" \
+    "$OUT/obj/kernels_gpu_const_fma.o" -lm -o "$OUT/srt_driver_fma"
+fi
+
 cp "$REF/GPU_program.cl" "$REF/CPU_program.cl" "$OUT/run_data/"
 cp "$REF"/unit_sphere_partitions/*.txt "$OUT/run_data/unit_sphere_partitions/"
-echo "build_ref: built $OUT/ref_const and $OUT/ref_var"
+echo "build_ref: built $OUT/ref_const, $OUT/ref_var and $OUT/srt_driver"

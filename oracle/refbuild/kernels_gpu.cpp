@@ -19,7 +19,7 @@ extern "C" void mockcl_register_kernel(const char* name, mockcl_tramp fn, int mo
 #define I(i) (*(const int*)args[i])
 
 // Argument lists follow the kernel signatures in GPU_program.cl:81-90,
-// 258-261, 292-295, 316-324, 626-628, 737-742.
+// 258-261, 292-295, 316-324, 626-628, 737-742, 868-874.
 static void t_pffls(void* const* args) {
   particle_fluid_forces_linear_stencil((int_param_struct*)A(0), (flp_param_struct*)A(1), (float*)A(2),
                                        (float*)A(3), (float4*)A(4), (float4*)A(5), (float4*)A(6), (float4*)A(7),
@@ -35,6 +35,13 @@ static void t_collide(void* const* args) {
   collideMRT_stream_D3Q19((float*)A(0), (float*)A(1), (float*)A(2), (float*)A(3), (float*)A(4), (int*)A(5),
                           (int_param_struct*)A(6), (flp_param_struct*)A(7));
 }
+// collideSRT_newtonian_stream_D3Q19 (GPU_program.cl:868-947): the reference's
+// BGK collide-stream kernel, which its host does not call; run by
+// srt_driver.c for the BGK golden vectors.
+static void t_srt(void* const* args) {
+  collideSRT_newtonian_stream_D3Q19((float*)A(0), (float*)A(1), (float*)A(2), (float*)A(3), (int_param_struct*)A(4),
+                                    (flp_param_struct*)A(5));
+}
 static void t_periodic(void* const* args) {
   boundary_periodic((float*)A(0), (int_param_struct*)A(1), (int*)A(2));
 }
@@ -47,6 +54,7 @@ __attribute__((constructor)) static void register_gpu_kernels() {
   mockcl_register_kernel("sum_particle_fluid_forces", t_sum, 0, 3);
   mockcl_register_kernel("reset_particle_fluid_forces", t_reset, 0, 3);
   mockcl_register_kernel("collideMRT_stream_D3Q19", t_collide, 0, 8);
+  mockcl_register_kernel("collideSRT_newtonian_stream_D3Q19", t_srt, 0, 6);
   mockcl_register_kernel("boundary_periodic", t_periodic, 0, 3);
   mockcl_register_kernel("boundary_velocity", t_velocity, 0, 5);
 }

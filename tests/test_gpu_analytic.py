@@ -29,7 +29,8 @@ pytestmark = pytest.mark.gpu
 NZ = 66
 
 
-def channel(model, g=0.0, U=0.0, tau=1.0, params=(0.0, 0.0, 0.0, 0.0), tau_max=0.0, casson_reg=0.0, arithmetic=0):
+def channel(model, g=0.0, U=0.0, tau=1.0, params=(0.0, 0.0, 0.0, 0.0), tau_max=0.0, casson_reg=0.0, arithmetic=0,
+            collision=0):
     kw = dict(iterations=10 ** 6, total_lattice_size=(8, 8, NZ), boundary_conditions_xyz=(0, 0, 1),
               velocity_bc_upper=(U, 0.0, 0.0), velocity_bc_lower=(-U, 0.0, 0.0), initial_f="constant",
               initial_vel=(0.0, 0.0, 0.0), domain_decomposition=(1, 1, 1), num_particles=0,
@@ -38,7 +39,7 @@ def channel(model, g=0.0, U=0.0, tau=1.0, params=(0.0, 0.0, 0.0, 0.0), tau_max=0
               tau_max=tau_max, casson_regularisation=casson_reg, rebuild_neigh_list_freq=10,
               video_freq=10 ** 9, shear_stress_freq=10 ** 9, console_print_freq=10 ** 9)
     hs = d3.HostState(d3.parse_config(d3.keywords_text(kw)))
-    return d3.Simulation.from_host_state(hs, arithmetic=arithmetic)
+    return d3.Simulation.from_host_state(hs, arithmetic=arithmetic, collision=collision)
 
 
 def steady_profile(sim, steps, check=5000):
