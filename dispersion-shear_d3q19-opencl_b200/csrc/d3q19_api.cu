@@ -1154,9 +1154,10 @@ extern "C" int d3q19_read_spread_force_static(d3q19_ctx* c, float* gpf0) {
   float* field = nullptr;
   int rc = spread_static_address(c, &field);
   if (rc) return rc;
-  cudaSetDevice(c->dev);
-  /* Nodes no marker reaches read 0, and the spread kernels add into the
-   * field: the used part starts at zero on every call. */
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  /* The spread kernels write the nodes of the tiles that have markers; every
+   * other node (tiles without markers, the buffer layer) must read 0, and the
+   * array still holds the last call's field: clear the used part first. */
   CUDA_TRY(c, cudaMemsetAsync(field, 0, sizeof(float) * 3 * NC, c->stream));
   if (c->ppar.np > 0) {
     TileLists tl;

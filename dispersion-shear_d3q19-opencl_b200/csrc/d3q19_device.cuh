@@ -367,7 +367,9 @@ __device__ __forceinline__ void collide(R (&f)[19], R rho, R ir, R ux, R uy, R u
   // (GPU_program.cl:978-1007): a fluid at rest then has exactly zero
   // non-equilibrium part, which the strain rate of a power-law or yield-
   // stress fluid at rest depends on.
-  const R r0 = rho / R(3.0f), r1 = rho / R(18.0f), r2 = rho / R(36.0f);
+  // rho/36 is rho/18 halved: a power-of-two scaling commutes with rounding,
+  // so it is the correctly rounded rho/36 without a second division.
+  const R r0 = rho / R(3.0f), r1 = rho / R(18.0f), r2 = R(0.5f) * r1;
   R d[19], base[19];
   {
     R feq0 = r0 * (R(1.0f) - usq15);

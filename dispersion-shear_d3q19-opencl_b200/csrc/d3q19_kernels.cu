@@ -523,8 +523,11 @@ __device__ __forceinline__ void particle_group(const ParticleArgs& a, const int 
     const int wg = grp - p * nfa;  // work-group of the sphere
     // The rigid-body update of the sphere, once per block and shared.
     const float4 r0 = l < L ? a.sphere[wg * L + l] : make_float4(0.f, 0.f, 0.f, 0.f);
-    // The marker template above is constant; the rigid-body update reads the
-    // contact forces of the side stream's pass, so it waits too.
+    // The marker template above is constant.  Everything after the wait reads
+    // the previous collide-stream pass's u and lists.  The contact forces of
+    // the side stream's pass, which the rigid-body update reads, are ordered
+    // by the host's stream wait on that pass's event before this launch, not
+    // by this wait (which orders only the preceding kernel of this stream).
     pdl_wait();
     pdl_trigger();
     if (l == 0) {

@@ -1,6 +1,6 @@
 """Generate the golden vectors in tests/golden/ from the reference itself.
 
-Runs the reference (built from /root/reference by oracle/refbuild/build_ref.sh
+Runs the reference (built from its source tree by oracle/refbuild/build_ref.sh
 into oracle/_ref/ and executed on the host through the mock OpenCL runtime,
 work-groups in order) for every case in cases.py, twice: with iterations=0
 to capture the initial state the reference's host builds, and with the

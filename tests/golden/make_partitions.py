@@ -15,7 +15,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("D3Q19_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_partitions.py <reference_dir> (or set D3Q19_REFERENCE)")
     d = os.path.join(ref, "unit_sphere_partitions")
     out = {}
     for fn in sorted(os.listdir(d)):
