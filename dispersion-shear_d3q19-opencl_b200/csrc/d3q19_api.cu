@@ -186,6 +186,10 @@ static int validate(const int_param_struct* ip, const flp_param_struct* fp, cons
     return fail(nullptr, D3Q19_EINVAL, "the FP64 build runs the reference's MRT on FP64 distributions only");
   if (o->arithmetic == 1 && o->collision != 0)
     return fail(nullptr, D3Q19_EINVAL, "the reference-exact arithmetic implements the reference's MRT only");
+  if (o->periodic_smoothing != 0 && o->periodic_smoothing != 1)
+    return fail(nullptr, D3Q19_EINVAL, "periodic_smoothing must be 0 or 1");
+  if (o->arithmetic == 1 && o->periodic_smoothing)
+    return fail(nullptr, D3Q19_EINVAL, "the reference-exact arithmetic smooths the force as the reference does");
   if (o->arithmetic == 1 && (o->tau_max != 0.0f || o->tau_min != 0.0f || o->casson_reg != 0.0f))
     return fail(nullptr, D3Q19_EINVAL, "the reference-exact arithmetic has the reference's tau limits only");
   if (o->arithmetic == 1 && (ip->MaxSurfPointsPerNode < 1 || ip->MaxSurfPointsPerNode > 16))
@@ -294,6 +298,7 @@ static int create_ctx(const int_param_struct* ip, const flp_param_struct* fp, co
   p.tauMin = o.tau_min;
   p.cassonReg = o.casson_reg;
   p.variable = o.variable_viscosity ? 1 : 0;
+  p.periodicSmooth = o.periodic_smoothing ? 1 : 0;
 
   ParticleParams& pp = c->ppar;
   memset(&pp, 0, sizeof(pp));
@@ -320,6 +325,7 @@ static int create_ctx(const int_param_struct* ip, const flp_param_struct* fp, co
   pp.tauN = fp->NewtonianTau;
   pp.fixed = o.fixed_particles ? 1 : 0;
   pp.exact = o.arithmetic == 1 ? 1 : 0;
+  pp.periodicSmooth = o.periodic_smoothing ? 1 : 0;
 
   const long long NC = g.NC;
   const size_t fbytes = (size_t)storage_bytes(o.storage) * 19 * NC;

@@ -574,9 +574,50 @@ __device__ __forceinline__ int fixed_exponent(unsigned fmax_bits) {
 // the two parts are summed exactly with 32-bit atomics, lo in the low word and
 // hi in the high word of the node's 64-bit slot; each sum is converted back
 // with one rounding.  Needs all FLUID_THREADS threads.
+// With periodic smoothing, the image of stencil node c on the periodic
+// buffer layer that the smoothing of its neighbours across the seam reads:
+// node N-2 also at 0, node 1 also at N-1; -1 for every other node.
+__device__ __forceinline__ int seam_image(int c, int N, bool wrap) {
+  return !wrap ? -1 : (c == N - 2 ? 0 : (c == 1 ? N - 1 : -1));
+}
+
+// Adds the fixed-point contribution c (already scaled by 2^k) of one stencil
+// node at halo coordinates (hx, hy, hz), if they lie in the halo.
+__device__ __forceinline__ void spread_add(SpreadSmem& s, int hx, int hy, int hz, const float (&c)[3], float scale,
+                                           unsigned* err) {
+  if (hx < 0 || hx >= HALO_X || hy < 0 || hy >= HALO_Y || hz < 0 || hz >= HALO_Z) return;
+  const int h = hx + HALO_X * (hy + HALO_Y * hz);
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const float sv = -c[d] * scale;  // exact: power-of-two scaling
+    if (!(fabsf(sv) < 549755813888.0f)) {  // 2^39
+      atomicOr(err, ERR_FIXED_RANGE);
+      continue;
+    }
+    const long long v = __float2ll_rn(sv);
+    unsigned* slot = reinterpret_cast<unsigned*>(&s.acc[d][h]);
+    atomicAdd(slot, (unsigned)(v & 0xffff));
+    atomicAdd(reinterpret_cast<int*>(slot + 1), (int)(v >> 16));
+  }
+}
+
+// Adds a stencil node (cx, cy, cz) of a marker to the tile's halo: the node
+// itself, and with periodic smoothing (wrap) its images on the periodic x/y
+// buffer layers.
+__device__ __forceinline__ void spread_node(SpreadSmem& s, const Geom& g, int cx, int cy, int cz, int X0, int Y0,
+                                            int Z0, bool wrap, const float (&c)[3], float scale, unsigned* err) {
+  const int hx = cx - (X0 - 1), hy = cy - (Y0 - 1), hz = cz - (Z0 - 1);
+  spread_add(s, hx, hy, hz, c, scale, err);
+  if (!wrap) return;
+  const int ix = seam_image(cx, g.Nx, g.periodic[0] != 0), iy = seam_image(cy, g.Ny, g.periodic[1] != 0);
+  if (ix >= 0) spread_add(s, ix - (X0 - 1), hy, hz, c, scale, err);
+  if (iy >= 0) spread_add(s, hx, iy - (Y0 - 1), hz, c, scale, err);
+  if (ix >= 0 && iy >= 0) spread_add(s, ix - (X0 - 1), iy - (Y0 - 1), hz, c, scale, err);
+}
+
 template <typename R = float>
 __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& tl, long long T, int n, int X0,
-                                int Y0, int Z0, int tid, int k, int first_id, unsigned* err) {
+                                int Y0, int Z0, int tid, int k, int first_id, unsigned* err, bool wrap = false) {
   float4 ma = make_float4(0.f, 0.f, 0.f, 0.f), mb = ma;
   if (tid < n && !out_of_bounds(first_id, tl.markers, err)) {  // issued before the clear: the round trip overlaps it
     ma = tl.mrec[2 * (long long)first_id];
@@ -607,22 +648,8 @@ __device__ void accumulate_tile(SpreadSmem& s, const Geom& g, const TileLists& t
                           {xs, ys, zs}};
 #pragma unroll
     for (int q = 0; q < 8; q++) {
-      const int hx = x0 + sh[q][0] - (X0 - 1), hy = y0 + sh[q][1] - (Y0 - 1), hz = z0 + sh[q][2] - (Z0 - 1);
-      if (hx < 0 || hx >= HALO_X || hy < 0 || hy >= HALO_Y || hz < 0 || hz >= HALO_Z) continue;
-      const int h = hx + HALO_X * (hy + HALO_Y * hz);
       const float c[3] = {w[q] * b.x, w[q] * b.y, w[q] * b.z};
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-        const float sv = -c[d] * scale;  // exact: power-of-two scaling
-        if (!(fabsf(sv) < 549755813888.0f)) {  // 2^39
-          atomicOr(err, ERR_FIXED_RANGE);
-          continue;
-        }
-        const long long v = __float2ll_rn(sv);
-        unsigned* slot = reinterpret_cast<unsigned*>(&s.acc[d][h]);
-        atomicAdd(slot, (unsigned)(v & 0xffff));
-        atomicAdd(reinterpret_cast<int*>(slot + 1), (int)(v >> 16));
-      }
+      spread_node(s, g, x0 + sh[q][0], y0 + sh[q][1], z0 + sh[q][2], X0, Y0, Z0, wrap, c, scale, err);
     }
   }
   __syncthreads();

@@ -56,6 +56,7 @@ struct FluidParams {
   float tauMin;         // lower clamp (the reference's MIN_TAU = 0.505)
   float cassonReg;      // 0 = none
   int variable;         // local tau (read only by kernels that choose the law at run time)
+  int periodicSmooth;   // the spread-force smoothing wraps across periodic x and y
 };
 
 // One IBM marker of the last particle pass, two float4 per marker:
@@ -106,6 +107,7 @@ struct ParticleParams {
   float zoneWidth[3];
   int fixed;
   int exact;  // contact forces summed in the reference's order
+  int periodicSmooth;  // list seam markers also in the tiles of their buffer-layer images
 };
 
 struct ParticleArgs {

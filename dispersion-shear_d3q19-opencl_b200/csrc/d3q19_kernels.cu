@@ -87,7 +87,7 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const int first, 
     }
     if (cnt > 0) {
       accumulate_tile<R>(sm, g, a.tiles, T, min(cnt, a.tiles.cap), X0, Y0, Z0, tid, fixed_exponent(fbits), first_id,
-                         a.err);
+                         a.err, a.p.periodicSmooth != 0);
       smooth_pair(sm, threadIdx.x, threadIdx.y, threadIdx.z, sg);
     }
   }
@@ -387,8 +387,20 @@ __device__ __forceinline__ void tile_range(int c, int T, int nt, int& lo, int& h
   if (hi > nt - 1) hi = nt - 1;
 }
 
-// Distinct tile indices covering two node coordinates (at most 4).
-__device__ __forceinline__ int tile_set(int c0, int c1, int T, int nt, int (&out)[4]) {
+// Distinct tile indices covering two node coordinates (at most 4).  With
+// wrap (periodic smoothing of the spread force on a periodic axis of N
+// nodes), also the tiles holding the buffer-layer images of stencil nodes on
+// the seam, which those tiles' smoothing reads.
+__device__ __forceinline__ void tile_add(int c, int T, int nt, int (&out)[4], int& n) {
+  int lo, hi;
+  tile_range(c, T, nt, lo, hi);
+  for (int t = lo; t <= hi && n < 4; t++) {
+    bool dup = false;
+    for (int j = 0; j < n; j++) dup |= out[j] == t;
+    if (!dup) out[n++] = t;
+  }
+}
+__device__ __forceinline__ int tile_set(int c0, int c1, int T, int nt, int (&out)[4], int N = 0, bool wrap = false) {
   int l0, h0, l1, h1, n = 0;
   tile_range(c0, T, nt, l0, h0);
   tile_range(c1, T, nt, l1, h1);
@@ -397,6 +409,11 @@ __device__ __forceinline__ int tile_set(int c0, int c1, int T, int nt, int (&out
     bool dup = false;
     for (int j = 0; j < n; j++) dup |= out[j] == t;
     if (!dup) out[n++] = t;
+  }
+  if (wrap) {
+    const int i0 = seam_image(c0, N, true), i1 = seam_image(c1, N, true);
+    if (i0 >= 0) tile_add(i0, T, nt, out, n);
+    if (i1 >= 0) tile_add(i1, T, nt, out, n);
   }
   return n;
 }
@@ -583,8 +600,8 @@ __device__ __forceinline__ void particle_group(const ParticleArgs& a, const int 
         torque = f4cross(r0, force);
         a.mrec[2 * gid] = make_float4(wx, wy, wz, __uint_as_float((unsigned)x0 | ((unsigned)y0 << 16)));
         a.mrec[2 * gid + 1] = make_float4(force.x, force.y, force.z, __uint_as_float((unsigned)z0));
-        nx = tile_set(x0, x0 + xs, TILE_X, g.ntx, tx);
-        ny = tile_set(y0, y0 + ys, TILE_Y, g.nty, ty);
+        nx = tile_set(x0, x0 + xs, TILE_X, g.ntx, tx, g.Nx, P.periodicSmooth && g.periodic[0]);
+        ny = tile_set(y0, y0 + ys, TILE_Y, g.nty, ty, g.Ny, P.periodicSmooth && g.periodic[1]);
         nz = tile_set(z0, z0 + zs, TILE_Z, g.ntz, tz);
       }
     }
@@ -753,8 +770,8 @@ __device__ __forceinline__ void particle_group_f64(const ParticleArgs& a, const 
       torque = d4cross(r0, force);
       a.mrec[2 * gid] = make_float4((float)wx, (float)wy, (float)wz, __uint_as_float((unsigned)x0 | ((unsigned)y0 << 16)));
       a.mrec[2 * gid + 1] = make_float4((float)force.x, (float)force.y, (float)force.z, __uint_as_float((unsigned)z0));
-      nx = tile_set(x0, x0 + xs, TILE_X, g.ntx, tx);
-      ny = tile_set(y0, y0 + ys, TILE_Y, g.nty, ty);
+      nx = tile_set(x0, x0 + xs, TILE_X, g.ntx, tx, g.Nx, P.periodicSmooth && g.periodic[0]);
+      ny = tile_set(y0, y0 + ys, TILE_Y, g.nty, ty, g.Ny, P.periodicSmooth && g.periodic[1]);
       nz = tile_set(z0, z0 + zs, TILE_Z, g.ntz, tz);
     }
   }

@@ -175,7 +175,8 @@ __device__ __forceinline__ void tma_issue_tile(unsigned char* stage, uint64_t* b
 // accumulation is (list entry j/8, stencil corner j%8).
 template <typename R>
 __device__ __forceinline__ void tma_tile_force(SpreadSmem& s, const Geom& g, const TileLists& tl, long long T, int n,
-                                               int X0, int Y0, int Z0, int tid, int k, unsigned* err, R (&sg)[3]) {
+                                               int X0, int Y0, int Z0, int tid, int k, unsigned* err, bool wrap,
+                                               R (&sg)[3]) {
   {
     int4* z4 = reinterpret_cast<int4*>(&s.acc[0][0]);
     for (int h = tid; h < 3 * HALO_N / 2; h += TMA_THREADS) z4[h] = make_int4(0, 0, 0, 0);
@@ -196,23 +197,9 @@ __device__ __forceinline__ void tma_tile_force(SpreadSmem& s, const Geom& g, con
     const int xs = (x0 == g.Nx - 2) ? -(g.Nx - 3) : 1;
     const int ys = (y0 == g.Ny - 2) ? -(g.Ny - 3) : 1;
     const int zs = (z0 == g.Nz - 2) ? -(g.Nz - 3) : 1;
-    const int hx = x0 + (sx ? xs : 0) - (X0 - 1), hy = y0 + (sy ? ys : 0) - (Y0 - 1), hz = z0 + (sz ? zs : 0) - (Z0 - 1);
-    if (hx < 0 || hx >= HALO_X || hy < 0 || hy >= HALO_Y || hz < 0 || hz >= HALO_Z) continue;
     const float w = (sx ? 1.0f - a.x : a.x) * (sy ? 1.0f - a.y : a.y) * (sz ? 1.0f - a.z : a.z);
-    const int h = hx + HALO_X * (hy + HALO_Y * hz);
     const float cf[3] = {w * b.x, w * b.y, w * b.z};
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      const float sv = -cf[d] * scale;  // exact: power-of-two scaling
-      if (!(fabsf(sv) < 549755813888.0f)) {  // 2^39
-        atomicOr(err, ERR_FIXED_RANGE);
-        continue;
-      }
-      const long long v = __float2ll_rn(sv);
-      unsigned* slot = reinterpret_cast<unsigned*>(&s.acc[d][h]);
-      atomicAdd(slot, (unsigned)(v & 0xffff));
-      atomicAdd(reinterpret_cast<int*>(slot + 1), (int)(v >> 16));
-    }
+    spread_node(s, g, x0 + (sx ? xs : 0), y0 + (sy ? ys : 0), z0 + (sz ? zs : 0), X0, Y0, Z0, wrap, cf, scale, err);
   }
   __syncthreads();
   // value = (hi * 2^16 + lo) * 2^-k; all sums are read before the field
@@ -373,7 +360,7 @@ __global__ void __launch_bounds__(TMA_THREADS, TMA_MIN_BLOCKS)
       }
       if (cnt > 0)
         tma_tile_force<R>(sp, g, a.tiles, T, min(cnt, a.tiles.cap), X0, Y0, Z0, tid, fixed_exponent(fbits), a.err,
-                          sg);
+                          a.p.periodicSmooth != 0, sg);
     }
 
     // The tile's populations.  One thread waits on the stage's barrier (its

@@ -57,7 +57,7 @@ class Options(C.Structure):
                 ("rebuild_freq", C.c_int), ("tangential_vel_bc", C.c_int * 3), ("tau_max", C.c_float),
                 ("tau_min", C.c_float), ("casson_reg", C.c_float), ("device", C.c_int),
                 ("ibm_tile_capacity", C.c_int), ("arithmetic", C.c_int), ("inplace", C.c_int),
-                ("fluid_kernel", C.c_int)]
+                ("fluid_kernel", C.c_int), ("periodic_smoothing", C.c_int)]
 
 
 class DeviceInfo(C.Structure):
@@ -75,7 +75,7 @@ class HostParams(C.Structure):
                 ("ParticleSeed", C.c_uint), ("MinParticleGap", C.c_float), ("TauMax", C.c_float),
                 ("TauMin", C.c_float), ("CassonReg", C.c_float), ("Collision", C.c_int), ("Storage", C.c_int),
                 ("ParticlePrecision", C.c_int), ("Arithmetic", C.c_int), ("Fp64Build", C.c_int),
-                ("Inplace", C.c_int)]
+                ("Inplace", C.c_int), ("PeriodicSmoothing", C.c_int)]
 
 
 class Config(C.Structure):

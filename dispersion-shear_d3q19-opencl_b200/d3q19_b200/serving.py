@@ -56,7 +56,10 @@ def solve_keywords(req: ShearRequest) -> dict:
     # so markers stay off the wall planes (a marker that crosses one wraps to
     # the other wall, as in the reference); sphere centres start in the slab
     # beyond it, and phi is the volume fraction of that slab (random
-    # sequential addition jams near 0.38).
+    # sequential addition jams near 0.38).  The force smoothing wraps across
+    # the periodic x/y seams (periodic_force_smoothing): with the reference's
+    # smoothing a sphere on a seam loses part of its reaction on the fluid,
+    # and dense suspensions build up velocity there until they diverge.
     zb = r + 2.0
     slab = (N[0] - 2) * (N[1] - 2) * max(N[2] - 2 - 2 * zb, 0.0)
     nsph = int(round(req.phi * slab / (4.0 / 3.0 * math.pi * r ** 3)))
@@ -64,7 +67,7 @@ def solve_keywords(req: ShearRequest) -> dict:
               velocity_bc_upper=(req.wall_speed, 0.0, 0.0), velocity_bc_lower=(-req.wall_speed, 0.0, 0.0),
               initial_f="constant", initial_vel=(0.0, 0.0, 0.0), domain_decomposition=(1, 1, 1),
               rebuild_neigh_list_freq=10, video_freq=10 ** 9, shear_stress_freq=10 ** 9, console_print_freq=10 ** 9,
-              num_particles=nsph)
+              num_particles=nsph, periodic_force_smoothing=1)
     if nsph > 0:
         kw.update(particle_diameter=req.diameter, initial_particle_distribution=4, particle_seed=req.seed,
                   min_particle_gap=0.0, initial_particle_buffer=0.0, z_wall_particle_buffer=zb,

@@ -83,6 +83,7 @@ static const keyword_t KEYWORDS[] = {
     {"reference_arithmetic", T_INT, HPO(Arithmetic), "0"},
     {"fp64_build", T_INT, HPO(Fp64Build), "0"},
     {"inplace_streaming", T_INT, HPO(Inplace), "0"},
+    {"periodic_force_smoothing", T_INT, HPO(PeriodicSmoothing), "0"},
 };
 #define NKEYWORDS ((int)(sizeof(KEYWORDS) / sizeof(KEYWORDS[0])))
 
@@ -718,5 +719,6 @@ void d3q19h_options(const d3q19h_config* cfg, d3q19_options* o) {
   o->tau_min = cfg->hp.TauMin;
   o->arithmetic = cfg->hp.Fp64Build ? 2 : cfg->hp.Arithmetic;
   o->inplace = cfg->hp.Inplace;
+  o->periodic_smoothing = cfg->hp.PeriodicSmoothing;
   o->casson_reg = cfg->hp.CassonReg;
 }

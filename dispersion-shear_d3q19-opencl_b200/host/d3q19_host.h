@@ -51,6 +51,7 @@ typedef struct {
   int Arithmetic;             /* reference_arithmetic: 1 = the reference's evaluation order */
   int Fp64Build;              /* fp64_build: 1 = the FP64 build of the fast kernels (arithmetic 2) */
   int Inplace;                /* inplace_streaming: 1 = one distribution buffer (AA pattern) */
+  int PeriodicSmoothing;      /* periodic_force_smoothing: 1 = the force smoothing wraps across periodic axes */
 } d3q19h_host_params;
 
 typedef struct {

@@ -152,6 +152,15 @@ typedef struct {
    * by instruction issue, which staging the loads does not reduce.  No
    * counterpart in the reference. */
   int fluid_kernel;
+  /* 0: the reference's 27-point smoothing of the spread force, which reads
+   * the buffer layer as zero and does not wrap across periodic axes
+   * (GPU_program.cl:356-377): a sphere on a periodic seam loses the part of
+   * its reaction force that the smoothing would carry across the seam, and
+   * the fluid there gains momentum without a counterpart.  1: the smoothing
+   * wraps across periodic x and y, so the spread force on the fluid is the
+   * whole marker force.  Not with arithmetic 1.  No counterpart in the
+   * reference. */
+  int periodic_smoothing;
 } d3q19_options;
 
 typedef struct {

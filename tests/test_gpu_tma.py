@@ -90,7 +90,7 @@ def test_lattices_the_tma_kernel_does_not_take():
     s.close()
     req = sv.ShearRequest(rid=0, edge=(36, 32, 32), phi=0.0, model="newtonian", wall_speed=0.02, seed=1)
     for over, want in ((dict(), "tma"), (dict(storage=1), "tile"), (dict(collision=1), "tile"),
-                       (dict(arithmetic=1), "reference-order"), (dict(arithmetic=2), "tile")):
+                       (dict(arithmetic=1, periodic_smoothing=0), "reference-order"), (dict(arithmetic=2), "tile")):
         s = d3.Simulation.from_host_state(sv.host_state(req), fluid_kernel=TMA, **over)
         assert s.fluid_kernel == want, over
         s.close()
