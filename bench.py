@@ -1,13 +1,19 @@
 #!/usr/bin/env python
 """Throughput benchmark of the B200 D3Q19 LBM + IBM time step.
 
-Workload (default "dense-powerlaw-128"): the dense power-law suspension --
-128^3 lattice (126^3 interior nodes, z walls at +-0.05 lu/step, periodic x/y),
-200 freely moving spheres of diameter 16 with 512 IBM markers each placed by
-seeded random sequential addition with a 2 lu minimum gap (phi = 21.6 %),
-power-law fluid n = 0.6, k = 0.0105, local tau clamped to [0.55, 2.0].  A
-step is one full time step (collide-stream with boundaries, IBM, rigid
-bodies, particle contacts, zone rebuild every 10 steps).
+Workload (default "suspension-128"): the dense power-law suspension as the
+reference's own host expresses it -- 128^3 lattice (126^3 interior nodes, z
+walls at +-0.05 lu/step, periodic x/y), 200 freely moving spheres of diameter
+16 on the reference's jittered grid with its marker rule (1024 IBM markers
+each), power-law fluid n = 0.6, k = 0.0105 with the reference's tau limits.
+Both arms (--impl ours and --impl reference) run it from the same keywords and
+initial state.  "dense-powerlaw-128" is the same lattice and sphere count with
+512 markers per sphere placed by seeded random sequential addition (2 lu gap)
+and tau clamped to [0.55, 2.0], which the reference's host cannot express; its
+reference arm is the C restatement of the reference's algorithm on the same
+initial state.  A step is one full time step (collide-stream with
+boundaries, IBM, rigid bodies, particle contacts, zone rebuild every 10
+steps).
 
 Metric: MLUPS = interior nodes x steps / s / 1e6, summed over GPUs (each GPU
 runs an independent replica: weak scaling, no collective on the data path).
@@ -94,6 +100,16 @@ REFERENCE_KEYWORDS = {
 
 
 REFERENCE_KEYWORDS["powerlaw-128-fluid"] = dict(REFERENCE_KEYWORDS["dense-powerlaw-128"], num_particles=0)
+# The dense suspension exactly as the reference's host expresses it -- its
+# marker rule (1024 points for d = 16), jittered-grid placement, its tau
+# limits -- run by both arms from the same keywords (the default line): the
+# 128^3 lattice, 200 spheres of d = 16, power law n = 0.6, walls +-0.05.
+REFERENCE_KEYWORDS["suspension-128"] = dict(REFERENCE_KEYWORDS["dense-powerlaw-128"], random_particle_shift=0.5,
+                                            iterations=10000, use_constant_viscosity=0)
+WORKLOADS["suspension-128"] = dict(REFERENCE_KEYWORDS["suspension-128"])
+DESCRIPTION["suspension-128"] = ("dense power-law suspension as the reference expresses it: 128^3 lattice, 200 spheres "
+                                 "d=16 on the reference's jittered grid (shift 0.5), 1024 markers each (the reference's "
+                                 "rule), n=0.6 k=0.0105 (the reference's tau limits), walls +-0.05")
 # The reference has no fixed spheres and derives 1024 markers for d = 16.
 REFERENCE_KEYWORDS["couette-sphere-64"] = dict(
     total_lattice_size=(64, 64, 64), boundary_conditions_xyz=(0, 0, 1), newtonian_tau=0.8, viscosity_model=1,
@@ -102,8 +118,10 @@ REFERENCE_KEYWORDS["couette-sphere-64"] = dict(
     initial_particle_buffer=31.0, z_wall_particle_buffer=2.0, domain_decomposition=(1, 1, 1),
     rebuild_neigh_list_freq=10, video_freq=1000000, shear_stress_freq=1000000, console_print_freq=1000000)
 # Which reference build runs the workload (with or without USE_CONSTANT_VISCOSITY).
-REFERENCE_VARIABLE = {"dense-powerlaw-128": True, "powerlaw-128-fluid": True, "couette-sphere-64": False}
+REFERENCE_VARIABLE = {"dense-powerlaw-128": True, "powerlaw-128-fluid": True, "couette-sphere-64": False,
+                      "suspension-128": True}
 REFERENCE_NOTE = {
+    "suspension-128": "the same keywords and initial state as the GPU arm (same_config)",
     "dense-powerlaw-128": "the 128^3 lattice with 200 d=16 spheres; reference marker rule (1024/sphere) and "
                           "jittered-grid placement",
     "powerlaw-128-fluid": "the 128^3 power-law lattice without spheres",
@@ -355,7 +373,8 @@ def run_ours(args, rank, world, local_rank, dist):
         "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": STORAGE[args.storage][2],
-        "data": "synthetic (seeded RSA placement)",
+        "data": ("synthetic (the reference's jittered-grid placement)" if args.workload == "suspension-128" else
+                 "synthetic (seeded RSA placement)" if args.workload == "dense-powerlaw-128" else "synthetic"),
         "impl": "ours",
         "config": {"workload": args.workload, "description": DESCRIPTION[args.workload],
                    "lattice": list(ip.LatticeSize), "interior_nodes": interior, "spheres": ip.NumParticles,
@@ -378,7 +397,11 @@ def run_ours(args, rank, world, local_rank, dist):
         "clocks": clk,
     }
     if world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args.workload)
+        if args.workload in PORT_WORKLOADS:
+            out["cpu_baseline"] = port_baseline(args.workload)
+            out["cpu_baseline"]["reference_program"] = cpu_baseline(args.workload)
+        else:
+            out["cpu_baseline"] = cpu_baseline(args.workload)
     return out
 
 
@@ -418,11 +441,62 @@ def cpu_baseline(workload, sample_steps=8):
             "sample": "oracle/_ref not built on this machine"}
 
 
+def port_baseline(workload, sample_steps=2):
+    """CPU throughput of the reference's algorithm on exactly the GPU arm's
+    initial state (lattice, sphere placement, markers): the C restatement
+    oracle/d3q19_oracle.c, pinned bit for bit to the reference's own program
+    on the golden vectors, run over the box's host cores (OpenMP over the
+    collide-stream loop).  The restatement follows the reference's tau limits
+    (no upper clamp), the GPU arm's configuration asks for tau in [0.55, 2]:
+    the same work per node."""
+    import numpy as np
+
+    from oracle import pyoracle as po
+
+    import d3q19_b200 as d3
+
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    hs = d3.HostState(d3.parse_config(d3.keywords_text(WORKLOADS[workload])), data_dir=os.getcwd())
+    ip, fp = hs.cfg.ip, hs.cfg.fp
+    nc = ip.LatticeSize[0] * ip.LatticeSize[1] * ip.LatticeSize[2]
+    oip, ofp = po.params_from_bytes(bytes(ip), bytes(fp))
+    sm = d3.periodic_map(ip)
+    arrays = dict(fA=hs.f.copy(), fB=hs.f.copy(), u=hs.u, tau_lb=hs.tau, strMap=sm, spherePoints=hs.spherePoints,
+                  zoneNeighDat=hs.zoneNeighDat, numParInZone=hs.numParInZone, numParInThread=hs.numParInThread,
+                  parsZone=hs.parsZone, zoneMembers=hs.zoneMembers, threadMembers=hs.threadMembers,
+                  parKin=hs.parKin, parForce=hs.parForce, parFluidForce=hs.parFluidForce,
+                  gpf=np.zeros(3 * max(ip.MaxSurfPointsPerNode, 1) * nc, np.float32),
+                  countPoint=np.zeros(nc, np.int32))
+    nth = hs.cfg.hp.DomainDecomp[0] * hs.cfg.hp.DomainDecomp[1] * hs.cfg.hp.DomainDecomp[2]
+    st = po.OracleState(oip, ofp, arrays, nth, hs.cfg.hp.RebuildFreq, not hs.cfg.hp.UseConstantViscosity)
+    st.step(1)  # first touch of the arrays
+    t0 = time.perf_counter()
+    st.run(2, sample_steps)
+    per = (time.perf_counter() - t0) / sample_steps
+    N = ip.LatticeSize
+    interior = (N[0] - 2) * (N[1] - 2) * (N[2] - 2)
+    return {"value": round(interior / per / 1e6, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": f"{sample_steps} steps (after one untimed step) of the reference's algorithm restated in C "
+                      f"(oracle/d3q19_oracle.c, bit-exact to the reference's own program on the golden vectors), "
+                      f"{threads} OpenMP threads, on the GPU arm's initial state: {DESCRIPTION[workload]}"}
+
+
+# Workloads whose reference arm is the restatement on the GPU arm's own state
+# (the reference's host cannot place spheres by seeded random sequential
+# addition or override its marker count).
+PORT_WORKLOADS = {"dense-powerlaw-128"}
+
+
 def run_reference_arm(args):
     if args.workload not in REFERENCE_KEYWORDS:
         return {"impl": "reference", "unavailable": f"{args.workload}: the reference runs one lattice per process and "
                                                     "has no pool or request loop"}
-    b = cpu_baseline(args.workload, sample_steps=max(1, min(args.steps, 8)))
+    if args.workload in PORT_WORKLOADS:
+        b = port_baseline(args.workload, sample_steps=max(1, min(args.steps, 2)))
+        b["reference_program"] = cpu_baseline(args.workload, sample_steps=max(1, min(args.steps, 8)))
+    else:
+        b = cpu_baseline(args.workload, sample_steps=max(1, min(args.steps, 8)))
     kw = WORKLOADS[args.workload]
     N = kw["total_lattice_size"]
     out = {"impl": "reference", "metric": "MLUPS", "value": b["value"], "unit": "MLUPS", "n_gpus": args.gpus,
@@ -744,7 +818,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="dense-powerlaw-128", choices=sorted(WORKLOADS) + ["batch-64",
+    ap.add_argument("--workload", default="suspension-128", choices=sorted(WORKLOADS) + ["batch-64",
                                                                                            "served-sweep",
                                                                                            "served-preempt",
                                                                                            "casson-precision"])
