@@ -297,6 +297,10 @@ def run_ours(args, rank, world, local_rank, dist):
     t += args.warmup
     sim.synchronize()
 
+    # The CUDA graphs the timed steps replay are captured (not run) first.
+    sim.prepare_run(t, args.steps)
+    sim.synchronize()
+
     # Timed region: exactly K steps, barrier + synchronize on both sides.
     clocks = ClockSampler(local_rank)
     if dist:

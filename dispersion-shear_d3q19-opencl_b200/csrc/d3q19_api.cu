@@ -774,54 +774,104 @@ extern "C" int d3q19_step(d3q19_ctx* c, int t) {
 
 static int gcd_i(int a, int b) { return b ? gcd_i(b, a % b) : a; }
 
+// The CUDA graph of L steps starting at step t with the context's current
+// buffer parities (captured on first use; the capture records the launches
+// without running them and leaves the context's state as it was).
+static int step_graph(d3q19_ctx* c, int t, int L, int Lp, cudaGraphExec_t* out) {
+  auto key = std::make_tuple(((t % Lp) + Lp) % Lp, c->cur, c->pcur, L);
+  auto it = c->graphs.find(key);
+  if (it == c->graphs.end()) {
+    int rc = join_side(c);
+    if (rc) return rc;
+    const int cur0 = c->cur, pcur0 = c->pcur, last0 = c->last_t;
+    cudaGraph_t graph;
+    CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < L && !rc; k++) rc = enqueue_step(c, t + k);
+    if (!rc) rc = join_side(c);
+    if (rc) {
+      cudaStreamEndCapture(c->stream, &graph);
+      c->side_pending = false;
+      return rc;
+    }
+    CUDA_TRY(c, cudaStreamEndCapture(c->stream, &graph));
+    cudaGraphExec_t exec;
+    CUDA_TRY(c, cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    it = c->graphs.emplace(key, exec).first;
+    c->cur = cur0;  // the capture only recorded the launches
+    c->pcur = pcur0;
+    c->last_t = last0;
+  }
+  *out = it->second;
+  return 0;
+}
+
+// The launch sequence repeats with period Lp in t (buffer parity and the
+// zone-rebuild schedule), so a captured chunk replays at any t with the same
+// phase and buffer assignment.  Chunks are CH steps; a shorter rest of at
+// least Lp steps replays a graph of the largest multiple of Lp when one was
+// captured before (d3q19_prepare_run), and steps one by one otherwise.
+static void run_schedule(const d3q19_ctx* c, int* Lp, int* CH) {
+  const int R = c->ppar.np > 0 ? c->opt.rebuild_freq : 2;
+  *Lp = 2 / gcd_i(2, R) * R;
+  *CH = *Lp * std::max(1, (64 + *Lp - 1) / *Lp);
+}
+
 extern "C" int d3q19_run(d3q19_ctx* c, int t0, int nsteps) {
   TRACE("d3q19_run");
   int rc = check_ready(c);
   if (rc) return rc;
   if (c->kstage != 0) return fail(c, D3Q19_ESTATE, "step %d was left between passes", c->kt);
   cudaSetDevice(c->dev);
-  // The launch sequence repeats with period Lp in t (buffer parity and the
-  // zone-rebuild schedule), so a captured chunk of CH steps replays at any
-  // t0 with the same phase and buffer assignment.
-  const int R = c->ppar.np > 0 ? c->opt.rebuild_freq : 2;
-  const int Lp = 2 / gcd_i(2, R) * R;
-  const int CH = Lp * std::max(1, (64 + Lp - 1) / Lp);
+  int Lp, CH;
+  run_schedule(c, &Lp, &CH);
   int t = t0, n = nsteps;
   while (n > 0) {
-    if (c->f_state != 2 || n < CH || c->profiling) {
+    int L = 0;
+    if (c->f_state == 2 && !c->profiling) {
+      if (n >= CH) {
+        L = CH;
+      } else if (n >= Lp) {
+        const int Ls = n / Lp * Lp;
+        if (c->graphs.count(std::make_tuple(((t % Lp) + Lp) % Lp, c->cur, c->pcur, Ls))) L = Ls;
+      }
+    }
+    if (L == 0) {
       if ((rc = enqueue_step(c, t))) return rc;
       t++;
       n--;
       continue;
     }
     if ((rc = join_side(c))) return rc;
-    auto key = std::make_tuple(((t % Lp) + Lp) % Lp, c->cur, c->pcur, CH);
-    auto it = c->graphs.find(key);
-    if (it == c->graphs.end()) {
-      const int cur0 = c->cur, pcur0 = c->pcur;
-      cudaGraph_t graph;
-      CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      for (int k = 0; k < CH && !rc; k++) rc = enqueue_step(c, t + k);
-      if (!rc) rc = join_side(c);
-      if (rc) {
-        cudaStreamEndCapture(c->stream, &graph);
-        c->side_pending = false;
-        return rc;
-      }
-      CUDA_TRY(c, cudaStreamEndCapture(c->stream, &graph));
-      cudaGraphExec_t exec;
-      CUDA_TRY(c, cudaGraphInstantiate(&exec, graph, 0));
-      cudaGraphDestroy(graph);
-      it = c->graphs.emplace(key, exec).first;
-      c->cur = cur0;  // capture only recorded the launches
-      c->pcur = pcur0;
-    }
-    CUDA_TRY(c, cudaGraphLaunch(it->second, c->stream));
-    // CH is even: buffer assignment is unchanged after the chunk.
-    t += CH;
-    n -= CH;
+    cudaGraphExec_t exec;
+    if ((rc = step_graph(c, t, L, Lp, &exec))) return rc;
+    CUDA_TRY(c, cudaGraphLaunch(exec, c->stream));
+    // L is even: the buffer assignment is unchanged after the chunk.
+    t += L;
+    n -= L;
+    c->last_t = t - 1;
   }
   return join_side(c);
+}
+
+extern "C" int d3q19_prepare_run(d3q19_ctx* c, int t0, int nsteps) {
+  TRACE("d3q19_prepare_run");
+  int rc = check_ready(c);
+  if (rc) return rc;
+  if (c->kstage != 0) return fail(c, D3Q19_ESTATE, "step %d was left between passes", c->kt);
+  if (c->f_state != 2) return 0;  // the first step after an upload runs one by one; prepare after it
+  cudaSetDevice(c->dev);
+  int Lp, CH;
+  run_schedule(c, &Lp, &CH);
+  int t = t0, n = nsteps;
+  while (n >= Lp) {
+    const int L = n >= CH ? CH : n / Lp * Lp;
+    cudaGraphExec_t exec;
+    if ((rc = step_graph(c, t, L, Lp, &exec))) return rc;
+    t += L;
+    n -= L;
+  }
+  return 0;
 }
 
 static int device_errors(d3q19_ctx* c) {

@@ -351,6 +351,11 @@ class Simulation:
     def run(self, t0: int, n: int):
         self._check(self.lib.d3q19_run(self.h, t0, n), "run")
 
+    def prepare_run(self, t0: int, n: int):
+        """Captures the CUDA graphs run(t0, n) replays without running them
+        (d3q19_prepare_run)."""
+        self._check(self.lib.d3q19_prepare_run(self.h, t0, n), "prepare_run")
+
     def synchronize(self):
         self._check(self.lib.d3q19_synchronize(self.h), "synchronize")
 

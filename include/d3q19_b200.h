@@ -244,8 +244,19 @@ int d3q19_k_particles(d3q19_ctx* ctx, int t);
 int d3q19_k_contacts(d3q19_ctx* ctx, int t);
 int d3q19_k_zones(d3q19_ctx* ctx);
 
-/* Steps t0 .. t0+nsteps-1, replayed from captured CUDA graphs. */
+/* Steps t0 .. t0+nsteps-1, replayed from captured CUDA graphs: chunks of
+ * about 64 steps (a multiple of the step schedule's period, lcm(2,
+ * rebuild_neigh_list_freq)) are captured on first use; a shorter rest of at
+ * least one period replays a graph captured before by d3q19_prepare_run, and
+ * steps one by one otherwise. */
 int d3q19_run(d3q19_ctx* ctx, int t0, int nsteps);
+
+/* Captures, without running them, the CUDA graphs a later
+ * d3q19_run(ctx, t0, nsteps) replays (with the context's state unchanged),
+ * so that the run itself launches no capture: a short run then replays
+ * graphs instead of stepping one by one.  Does nothing before the first step
+ * after an upload.  No counterpart in the reference. */
+int d3q19_prepare_run(d3q19_ctx* ctx, int t0, int nsteps);
 
 /* clFinish (sim_main.c:407, 447): waits for the stream and reports device
  * errors (tile overflow, non-finite values). */

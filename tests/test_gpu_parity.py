@@ -190,3 +190,26 @@ def test_pass_by_pass_steps_match_step():
         b.step(26)
     a.close()
     b.close()
+
+
+def test_prepared_short_run_matches_eager_steps():
+    """A run shorter than a graph chunk replays the graph d3q19_prepare_run
+    captured (one period of the step schedule and more) and ends in the same
+    state as stepping one by one; preparing leaves the state unchanged."""
+    case = CASES["contacts"]
+    g = load_golden("contacts")
+    a, ip, _ = sim_from_golden(g, case)
+    b, _, _ = sim_from_golden(g, case)
+    a.run(1, 3)
+    b.run(1, 3)
+    a.prepare_run(4, 25)  # 20 steps from a graph (two periods of 10), 5 one by one
+    a.run(4, 25)
+    a.run(29, 5)
+    a.run(34, 20)  # the same phase and buffer parities as at step 4: the graph again
+    for t in range(4, 54):
+        b.step(t)
+    for rd in ("read_u", "read_f", "read_parkin", "read_parfluidforce", "read_parforce"):
+        x, y = getattr(a, rd)(), getattr(b, rd)()
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), rd
+    a.close()
+    b.close()
