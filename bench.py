@@ -578,19 +578,20 @@ def run_batch(args):
     for hs in states:
         if pool.admit(hs) is None:
             raise RuntimeError("batch does not fit the pool")
-    # Autotuner: persistent grid sizes (CTAs per SM of the fluid, particle and
-    # contact passes), each timed on a 200-step chunk of the live batch (the
-    # results do not depend on the grid); the fastest is kept.
-    sms = torch.cuda.get_device_properties(0).multi_processor_count
-    trials = []
-    for fb in (2, 3, 4):
-        for pb in (1, 2, 4):
-            pool.set_grid(fb * sms, pb * sms, pb * sms)
-            pool.advance(200)  # capture
-            trials.append((_time_pool(pool, 200, pool.stream_ptr, torch), fb, pb))
-    best = min(trials)
-    pool.set_grid(best[1] * sms, best[2] * sms, best[2] * sms)
+    # The library's grid autotuner (d3q19_pool_autotune): each 200-step
+    # advance of the live batch times the next candidate grid of the batch's
+    # work class until every candidate has run; the fastest is kept.  The
+    # results do not depend on the grid, so these are ordinary steps.
+    d3.tune_clear()
+    tuning_steps = 0
+    while not pool.tune_state()["settled"]:
+        pool.advance(200)
+        tuning_steps += 200
+    trials = pool.tune_trials()
+    best = min(trials, key=lambda x: x[2])
     pool.advance(chunk)  # capture of the 1000-step chunk
+    grid = pool.get_grid()[:2]
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
     ms = _time_pool(pool, chunk * max(1, args.steps // chunk), pool.stream_ptr, torch)
     steps = chunk * max(1, args.steps // chunk)
     pool.close()
@@ -617,8 +618,11 @@ def run_batch(args):
             "config": {"workload": "batch-64", "boxes": len(states), "interior_nodes": nodes,
                        "description": "64 boxes, edges from {32,48,64,96} per axis, 1-20 spheres of radius 4-8, "
                                       "power-law n in [0.4,1], walls +-[0.01,0.05]; one launch per pass for all"},
-            "autotune": {"fluid_ctas_per_sm": best[1], "particle_ctas_per_sm": best[2],
-                         "trials_ms_per_200_steps": [[round(t, 3), f, pp] for t, f, pp in trials]},
+            "autotune": {"fluid_ctas_per_sm": best[0], "particle_ctas_per_sm": best[1],
+                         "grid_in_use": [g // sms for g in grid], "tuning_steps": tuning_steps,
+                         "default_grid": [4, 4],
+                         "trials_ns_per_tile_step": [[f, pp, round(t, 2)] for f, pp, t in trials],
+                         "tile": "32x4x4"},
             "one_at_a_time_fp32": {"value": round(alone, 1), "unit": "MLUPS"},
             "speedup_vs_one_at_a_time_fp32": round(batched / alone, 2)}
 
@@ -652,14 +656,17 @@ def run_served(args):
     from d3q19_b200 import serving as sv
 
     torch.cuda.set_device(0)
-    reqs = sv.make_requests(args.requests, 50.0, 2024, edges=(32, 64))
-    max_steps = 40000
+    reqs = sv.make_requests(args.requests, 50.0, 2024, edges=tuple(args.edges))
+    max_steps = args.max_steps
     warm_served_paths((0, 1))
     runs = {}
     for storage in (0, 1):
         pool = d3.Pool(storage=storage, max_slots=256, hbm_budget=100 << 30, inplace=args.inplace)
         runs[storage] = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=max_steps).run(reqs)
         pool.close()
+    # The autotuner's choices for the work classes the pools met (CTAs per SM
+    # of the fluid and particle passes, ns per fluid tile step).
+    tuned = [ln.split("\t") for ln in d3.tune_export().splitlines()]
     served, served16 = sv.summary(*runs[0]), sv.summary(*runs[1])
     base, bwall = sv.one_at_a_time(reqs, storage=0, check_every=500, rel_tol=1e-4, max_steps=max_steps)
     alone = sv.summary(base, bwall)
@@ -675,9 +682,13 @@ def run_served(args):
             "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
             "data": "synthetic (seeded Poisson arrivals)", "impl": "ours",
             "config": {"workload": "served-sweep", "requests": len(reqs), "arrival_rate_per_s": 50.0,
-                       "edges": [32, 64], "phi": [0.0, 0.3], "models": list(sv.MODELS), "stop": "1e-4 over 500 steps",
+                       "edges": list(args.edges), "phi": [0.0, 0.3], "models": list(sv.MODELS),
+                       "stop": "1e-4 over 500 steps",
                        "max_steps": max_steps, "pool_storage": "fp32",
                        "pool_layout": "in place" if args.inplace else "two buffers"},
+            "autotune": [{"storage": int(t[2]), "inplace": int(t[3]), "class_tiles": f"<2^{t[4]}",
+                          "fluid_ctas_per_sm": int(t[5]), "particle_ctas_per_sm": int(t[6]),
+                          "ns_per_tile_step": float(t[7])} for t in tuned],
             "served": served, "served_fp16_pool": served16, "one_at_a_time_fp32": alone,
             "speedup_solves_per_s": round(served["solves_per_s"] / alone["solves_per_s"], 2),
             "speedup_fp16_pool": round(served16["solves_per_s"] / alone["solves_per_s"], 2),
@@ -827,6 +838,9 @@ def main():
                                                                                            "served-preempt",
                                                                                            "casson-precision"])
     ap.add_argument("--requests", type=int, default=128, help="served-sweep: number of requests")
+    ap.add_argument("--edges", type=int, nargs=2, default=[32, 64], metavar=("LO", "HI"),
+                    help="served-sweep: range of the cubic edges drawn")
+    ap.add_argument("--max-steps", type=int, default=40000, help="served-sweep: step cap of a solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fluid-kernel", default="tile", choices=sorted(FLUID_KERNELS),
                     help="collide-stream kernel: tile (the per-tile kernel) or tma (the TMA-pipelined kernel "

@@ -1506,6 +1506,15 @@ struct d3q19_pool {
   size_t stats_cap = 0;
   std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> graphs;  // (steps, fblocks, pblocks, cblocks, inplace)
   long long steps = 0;
+  // Grid autotuner (d3q19_pool_autotune): on or off, and the advance being
+  // timed (its table key, candidate and fluid tile steps), if any.
+  bool tune = false;
+  bool tune_pending = false;
+  std::string tune_key;
+  int tune_cand = -1;
+  double tune_units = 0;
+  cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
+  char dev_name[256] = {0};
   // Every d3q19_pool_* call holds it: the pool may be driven from several
   // host threads (its members are not stepped outside these calls).
   std::mutex mu;
@@ -1559,7 +1568,10 @@ extern "C" int d3q19_pool_create(int device, int storage, int rebuild_freq, int 
   // Persistent grids: blocks per SM the kernels' register and shared memory
   // bounds allow (the autotuner may lower them).
   p->sm_count = pr.multiProcessorCount;
-  p->fblocks = pr.multiProcessorCount * (storage == STORE_F32 ? 5 : 4);
+  snprintf(p->dev_name, sizeof(p->dev_name), "%s", pr.name);
+  for (char* q = p->dev_name; *q; q++)  // the name is a field of the tuning table's lines
+    if (*q == '\t' || *q == '\n' || *q == '|') *q = ' ';
+  p->fblocks = pr.multiProcessorCount * (storage == STORE_F32 ? 5 : 4) * FLUID_CTA_SCALE;
   p->pblocks = pr.multiProcessorCount * 4;
   p->cblocks = pr.multiProcessorCount * 4;
   cudaMemPoolProps mp;
@@ -1570,6 +1582,7 @@ extern "C" int d3q19_pool_create(int device, int storage, int rebuild_freq, int 
   const unsigned long long keep = ~0ull;
   if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&p->ev_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&p->ev_t0) != cudaSuccess || cudaEventCreate(&p->ev_t1) != cudaSuccess ||
       cudaMemPoolCreate(&p->mempool, &mp) != cudaSuccess ||
       cudaMemPoolSetAttribute(p->mempool, cudaMemPoolAttrReleaseThreshold, (void*)&keep) != cudaSuccess ||
       cudaMalloc(&p->d_fargs, sizeof(FluidArgs) * 2 * max_slots) != cudaSuccess ||
@@ -1745,7 +1758,7 @@ static int pool_enqueue(d3q19_pool* p, int nsteps) {
     // In place, the FP32 kernels run 4 blocks/SM: a larger persistent grid
     // would only add a second wave.
     const int aa = p->inplace == 1 ? (par == 0 ? 1 : 2) : 0;
-    const int fb = aa && p->storage == STORE_F32 ? std::min(p->fblocks, 4 * p->sm_count) : p->fblocks;
+    const int fb = aa && p->storage == STORE_F32 ? std::min(p->fblocks, 4 * FLUID_CTA_SCALE * p->sm_count) : p->fblocks;
     POOL_TRY(p, launch_fluid_batch(p->d_fargs, fw, p->d_counts + 0, par, p->storage, aa, fb, p->stream));
     POOL_TRY(p, launch_particle_batch(p->d_pargs, pw, p->d_counts + 1, par, p->part_threads, p->pblocks, p->stream));
     POOL_TRY(p, launch_contact_batch(p->d_pargs, cw, p->d_counts + 2, par, p->cblocks, p->stream));
@@ -1753,6 +1766,97 @@ static int pool_enqueue(d3q19_pool* p, int nsteps) {
       POOL_TRY(p, launch_zone_batch(p->d_zargs, p->d_zslots, p->d_counts + 3, par, p->max_slots, p->stream));
   }
   return 0;
+}
+
+// ---- Persistent-grid autotuner ---------------------------------------------
+// A process-wide table, keyed by the device (name and SM count), the pool's
+// storage and layout, and the size class of its work (the bit length of the
+// fluid tile count).  An entry holds the candidate grids -- fluid CTAs per SM
+// by particle/contact CTAs per SM -- with the time each measured, in ns per
+// fluid tile step, and the fastest once every candidate has run.  The batched
+// kernels take their items from work lists, so results do not depend on the
+// grid: a timed advance is an ordinary advance of the members.
+struct TuneEntry {
+  std::vector<std::pair<int, int>> cand;  // (fluid, particle/contact) CTAs per SM
+  std::vector<double> cost;               // ns per fluid tile step; < 0 until timed
+  int best = -1;                          // index of the choice once settled
+};
+static std::mutex g_tune_mu;
+static std::map<std::string, TuneEntry> g_tune;
+// Advances shorter than this are not timed (launch overhead would dominate).
+constexpr int TUNE_MIN_STEPS = 100;
+
+static int tune_class(long long nf) {
+  int c = 0;
+  while (nf > 0) {
+    c++;
+    nf >>= 1;
+  }
+  return c;
+}
+
+static std::string tune_key_of(const char* dev_name, int sms, int storage, int inplace, int cls) {
+  char buf[400];
+  snprintf(buf, sizeof(buf), "%s\t%d\t%d\t%d\t%d", dev_name, sms, storage, inplace, cls);
+  return buf;
+}
+
+// The candidates of a pool: fluid 2..4 CTAs per SM (2..5 for the two-buffer
+// FP32 layout, whose register bound admits 5) by particle/contact 1, 2, 4.
+static TuneEntry tune_candidates(const d3q19_pool* p) {
+  TuneEntry e;
+  const int fmax = (p->storage == STORE_F32 && p->inplace != 1) ? 5 : 4;
+  for (int f = 2; f <= fmax; f++)
+    for (int q : {1, 2, 4}) e.cand.push_back({f * FLUID_CTA_SCALE, q});
+  e.cost.assign(e.cand.size(), -1.0);
+  return e;
+}
+
+// Records the time of the timed advance in flight, if any (waits for it).
+static int tune_collect(d3q19_pool* p) {
+  if (!p->tune_pending) return 0;
+  p->tune_pending = false;
+  POOL_TRY(p, cudaEventSynchronize(p->ev_t1));
+  float ms = 0.f;
+  POOL_TRY(p, cudaEventElapsedTime(&ms, p->ev_t0, p->ev_t1));
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(p->tune_key);
+  if (it == g_tune.end() || it->second.best >= 0 || p->tune_cand >= (int)it->second.cand.size()) return 0;
+  TuneEntry& e = it->second;
+  e.cost[p->tune_cand] = ms * 1e6 / p->tune_units;
+  int best = 0;
+  for (size_t i = 0; i < e.cost.size(); i++) {
+    if (e.cost[i] < 0) return 0;  // candidates left
+    if (e.cost[i] < e.cost[best]) best = (int)i;
+  }
+  e.best = best;
+  // The choice applies from now on (the next advance of this class uses it).
+  p->fblocks = e.cand[best].first * p->sm_count;
+  p->pblocks = p->cblocks = e.cand[best].second * p->sm_count;
+  return 0;
+}
+
+// Before an advance of nsteps: the grid of the pool's class, or the next
+// candidate to time.  Returns true when this advance is to be timed.
+static bool tune_choose(d3q19_pool* p, int nsteps) {
+  if (!p->tune || p->nf <= 0 || p->inplace < 0) return false;
+  const std::string key = tune_key_of(p->dev_name, p->sm_count, p->storage, p->inplace, tune_class(p->nf));
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(key);
+  if (it == g_tune.end()) it = g_tune.emplace(key, tune_candidates(p)).first;
+  const TuneEntry& e = it->second;
+  int c = e.best;
+  if (c < 0 && nsteps >= TUNE_MIN_STEPS)
+    for (c = 0; c < (int)e.cost.size() && e.cost[c] >= 0; c++) {
+    }
+  if (c < 0 || c >= (int)e.cand.size()) return false;
+  p->fblocks = e.cand[c].first * p->sm_count;
+  p->pblocks = p->cblocks = e.cand[c].second * p->sm_count;
+  if (e.best >= 0) return false;
+  p->tune_key = key;
+  p->tune_cand = c;
+  p->tune_units = (double)nsteps * (double)p->nf;
+  return true;
 }
 
 extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
@@ -1768,8 +1872,10 @@ extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
       POOL_TRY(p, cudaEventRecord(p->slot[s]->ev_fork, p->slot[s]->stream));
       POOL_TRY(p, cudaStreamWaitEvent(p->stream, p->slot[s]->ev_fork, 0));
     }
+  if (int rc = tune_collect(p)) return rc;
   if (p->dirty)
     if (int rc = pool_upload(p)) return rc;
+  const bool timed = tune_choose(p, nsteps);
   auto key = std::make_tuple(nsteps, p->fblocks, p->pblocks, p->cblocks, p->inplace);
   auto it = p->graphs.find(key);
   if (it == p->graphs.end()) {
@@ -1784,8 +1890,14 @@ extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return pfail(p, D3Q19_ECUDA, "pool graph: %s", cudaGetErrorString(e));
     it = p->graphs.emplace(key, exec).first;
+    POOL_TRY(p, cudaGraphUpload(exec, p->stream));  // not inside a timed advance
   }
+  if (timed) POOL_TRY(p, cudaEventRecord(p->ev_t0, p->stream));
   POOL_TRY(p, cudaGraphLaunch(it->second, p->stream));
+  if (timed) {
+    POOL_TRY(p, cudaEventRecord(p->ev_t1, p->stream));
+    p->tune_pending = true;
+  }
   POOL_TRY(p, cudaEventRecord(p->ev_done, p->stream));
   for (int s = 0; s < p->max_slots; s++) {
     d3q19_ctx* c = p->slot[s];
@@ -1971,6 +2083,121 @@ extern "C" int d3q19_pool_set_grid(d3q19_pool* p, int fluid_blocks, int particle
   p->fblocks = fluid_blocks;
   p->pblocks = particle_blocks;
   p->cblocks = contact_blocks;
+  p->tune = false;
+  return 0;
+}
+
+extern "C" int d3q19_pool_autotune(d3q19_pool* p, int enable) {
+  if (!p || (enable != 0 && enable != 1)) return D3Q19_EINVAL;
+  POOL_LOCK(p);
+  p->tune = enable != 0;
+  return 0;
+}
+
+// The table entry of the pool's current work class (under g_tune_mu), or null.
+static const TuneEntry* tune_entry_of(const d3q19_pool* p) {
+  if (p->nf <= 0 || p->inplace < 0) return nullptr;
+  auto it = g_tune.find(tune_key_of(p->dev_name, p->sm_count, p->storage, p->inplace, tune_class(p->nf)));
+  return it == g_tune.end() ? nullptr : &it->second;
+}
+
+extern "C" int d3q19_pool_tune_state(d3q19_pool* p, int* fluid_per_sm, int* particle_per_sm, int* settled,
+                                     int* tried, int* total) {
+  if (!p) return D3Q19_EINVAL;
+  POOL_LOCK(p);
+  cudaSetDevice(p->dev);
+  if (int rc = tune_collect(p)) return rc;
+  if (fluid_per_sm) *fluid_per_sm = p->fblocks / p->sm_count;
+  if (particle_per_sm) *particle_per_sm = p->pblocks / p->sm_count;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  const TuneEntry* e = tune_entry_of(p);
+  int n = 0;
+  if (e)
+    for (double c : e->cost) n += c >= 0;
+  if (settled) *settled = e && e->best >= 0;
+  if (tried) *tried = n;
+  if (total) *total = e ? (int)e->cand.size() : 0;
+  return 0;
+}
+
+extern "C" int d3q19_pool_tune_trials(d3q19_pool* p, int* fluid_per_sm, int* particle_per_sm, double* ns_per_tile_step,
+                                      int cap, int* n) {
+  if (!p || !n || cap < 0) return D3Q19_EINVAL;
+  POOL_LOCK(p);
+  cudaSetDevice(p->dev);
+  if (int rc = tune_collect(p)) return rc;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  const TuneEntry* e = tune_entry_of(p);
+  *n = e ? (int)e->cand.size() : 0;
+  for (int i = 0; i < *n && i < cap; i++) {
+    if (fluid_per_sm) fluid_per_sm[i] = e->cand[i].first;
+    if (particle_per_sm) particle_per_sm[i] = e->cand[i].second;
+    if (ns_per_tile_step) ns_per_tile_step[i] = e->cost[i];
+  }
+  return 0;
+}
+
+extern "C" int d3q19_tune_export(char* buf, size_t cap, size_t* len) {
+  if (!len || (cap && !buf)) return D3Q19_EINVAL;
+  std::string out;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    char line[96];
+    for (const auto& kv : g_tune) {
+      const TuneEntry& e = kv.second;
+      if (e.best < 0) continue;
+      snprintf(line, sizeof(line), "\t%d\t%d\t%.6g\n", e.cand[e.best].first, e.cand[e.best].second,
+               e.cost[e.best]);
+      out += kv.first;
+      out += line;
+    }
+  }
+  *len = out.size();
+  if (cap < out.size() + 1) return cap ? D3Q19_ENOMEM : 0;
+  memcpy(buf, out.c_str(), out.size() + 1);
+  return 0;
+}
+
+extern "C" int d3q19_tune_import(const char* text) {
+  if (!text) return D3Q19_EINVAL;
+  std::vector<std::pair<std::string, TuneEntry>> add;
+  const char* q = text;
+  while (*q) {
+    const char* eol = strchr(q, '\n');
+    const std::string line(q, eol ? (size_t)(eol - q) : strlen(q));
+    q = eol ? eol + 1 : q + line.size();
+    if (line.empty()) continue;
+    // name, SMs, storage, inplace, class: the key; then the choice and its time.
+    std::vector<std::string> fld;
+    size_t a = 0;
+    for (size_t b; (b = line.find('\t', a)) != std::string::npos; a = b + 1) fld.push_back(line.substr(a, b - a));
+    fld.push_back(line.substr(a));
+    if (fld.size() != 8 || fld[0].empty()) return D3Q19_EINVAL;
+    int v[6];
+    double ns = 0;
+    char* end = nullptr;
+    for (int i = 0; i < 6; i++) {
+      const long x = strtol(fld[1 + i].c_str(), &end, 10);
+      if (*end || fld[1 + i].empty() || x < 0 || x > 1000000) return D3Q19_EINVAL;
+      v[i] = (int)x;
+    }
+    ns = strtod(fld[7].c_str(), &end);
+    if (*end || fld[7].empty() || !(ns >= 0)) return D3Q19_EINVAL;
+    if (v[1] > 2 || v[2] > 1 || v[4] < 1 || v[5] < 1) return D3Q19_EINVAL;
+    TuneEntry e;
+    e.cand.push_back({v[4], v[5]});
+    e.cost.push_back(ns);
+    e.best = 0;
+    add.emplace_back(tune_key_of(fld[0].c_str(), v[0], v[1], v[2], v[3]), e);
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (auto& kv : add) g_tune[kv.first] = kv.second;
+  return 0;
+}
+
+extern "C" int d3q19_tune_clear(void) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.clear();
   return 0;
 }
 
@@ -2015,6 +2242,7 @@ extern "C" int d3q19_pool_destroy(d3q19_pool* p) {
   { POOL_LOCK(p); }
   cudaSetDevice(p->dev);
   if (p->stream) cudaStreamSynchronize(p->stream);
+  tune_collect(p);  // a timed advance still counts
   pool_drop_graphs(p);
   for (auto*& c : p->slot)
     if (c) {
@@ -2028,6 +2256,8 @@ extern "C" int d3q19_pool_destroy(d3q19_pool* p) {
   if (p->stream) cudaStreamSynchronize(p->stream);  // the members' stream-ordered frees
   if (p->mempool) cudaMemPoolDestroy(p->mempool);
   if (p->ev_done) cudaEventDestroy(p->ev_done);
+  if (p->ev_t0) cudaEventDestroy(p->ev_t0);
+  if (p->ev_t1) cudaEventDestroy(p->ev_t1);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
   return 0;

@@ -10,10 +10,22 @@ namespace d3q19 {
 // of 32 x-nodes (one warp) by TILE_Y rows by TILE_Z planes; the 256 threads
 // (32 x 4 x 2) take TILE_Z/2 planes each.  The IBM force of a tile is
 // accumulated over the tile plus a one-node halo.
+// D3Q19_TILE_Y: a build knob for measuring other tile heights (2, 4, 8).
+// Measured on B200 (collide-stream kernel ms; MLUPS of the batched pool):
+// 128^3 suspension 0.1100 (4) / 0.1165 (2) / 0.1145 (8); the same fluid
+// without spheres 0.0792 / 0.0777 / 0.0832; 64 batched boxes 16,704 /
+// 14,575 / 16,390 MLUPS.  4 is kept: 2 wins only the sphere-free lattice,
+// by 2 %.
+#ifndef D3Q19_TILE_Y
+#define D3Q19_TILE_Y 4
+#endif
 constexpr int TILE_X = 32;
-constexpr int TILE_Y = 4;
+constexpr int TILE_Y = D3Q19_TILE_Y;
 constexpr int TILE_Z = 4;
 constexpr int FLUID_THREADS = TILE_X * TILE_Y * 2;
+// Fluid CTAs per SM of the pool's persistent grids are counted in units of
+// 256 threads: a lower tile packs more CTAs on an SM.
+constexpr int FLUID_CTA_SCALE = FLUID_THREADS < 256 ? 256 / FLUID_THREADS : 1;
 constexpr int HALO_X = TILE_X + 2;
 constexpr int HALO_Y = TILE_Y + 2;
 constexpr int HALO_Z = TILE_Z + 2;

@@ -140,6 +140,12 @@ def cuda_lib():
         lib.d3q19_pool_usage.argtypes = [P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
         lib.d3q19_pool_set_grid.argtypes = [P, C.c_int, C.c_int, C.c_int]
         lib.d3q19_pool_get_grid.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        lib.d3q19_pool_autotune.argtypes = [P, C.c_int]
+        lib.d3q19_pool_tune_state.argtypes = [P] + [C.POINTER(C.c_int)] * 5
+        lib.d3q19_pool_tune_trials.argtypes = [P, P, P, P, C.c_int, C.POINTER(C.c_int)]
+        lib.d3q19_tune_export.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+        lib.d3q19_tune_import.argtypes = [C.c_char_p]
+        lib.d3q19_tune_clear.argtypes = []
         lib.d3q19_pool_synchronize.argtypes = [P]
         lib.d3q19_pool_poll.argtypes = [P]
         lib.d3q19_pool_stream.restype = P
@@ -483,18 +489,76 @@ def context_bytes(ip: IntParams, options: Options | None = None) -> int:
     return int(out.value)
 
 
+def tune_export() -> str:
+    """The settled classes of the grid autotuner's table (d3q19_tune_export)."""
+    lib = cuda_lib()
+    n = C.c_size_t()
+    rc = lib.d3q19_tune_export(None, 0, C.byref(n))
+    if rc:
+        raise D3Q19Error(f"d3q19_tune_export: {STATUS.get(rc, rc)}")
+    buf = C.create_string_buffer(n.value + 1)
+    rc = lib.d3q19_tune_export(buf, n.value + 1, C.byref(n))
+    if rc:
+        raise D3Q19Error(f"d3q19_tune_export: {STATUS.get(rc, rc)}")
+    return buf.value.decode()
+
+
+def tune_import(text: str):
+    """Adds settled classes to the autotuner's table (d3q19_tune_import)."""
+    rc = cuda_lib().d3q19_tune_import(text.encode())
+    if rc:
+        raise D3Q19Error(f"d3q19_tune_import: {STATUS.get(rc, rc)}")
+
+
+def tune_clear():
+    cuda_lib().d3q19_tune_clear()
+
+
+# D3Q19_TUNE_CACHE names a file that keeps the autotuner's table between
+# processes: read when the first pool is created, written when a pool closes.
+_TUNE_LOADED = False
+
+
+def _tune_cache_load():
+    global _TUNE_LOADED
+    path = os.environ.get("D3Q19_TUNE_CACHE")
+    if _TUNE_LOADED or not path:
+        return
+    _TUNE_LOADED = True
+    if os.path.exists(path):
+        with open(path) as fh:
+            tune_import(fh.read())
+
+
+def _tune_cache_save():
+    path = os.environ.get("D3Q19_TUNE_CACHE")
+    if path:
+        text = tune_export()
+        tmp = f"{path}.{os.getpid()}.tmp"
+        with open(tmp, "w") as fh:
+            fh.write(text)
+        os.replace(tmp, path)
+
+
 class Pool:
     """Many independent shear cells resident on one GPU, advanced together in
-    batched persistent kernels (d3q19_pool_* of the C ABI)."""
+    batched persistent kernels (d3q19_pool_* of the C ABI).
+
+    autotune: the persistent grid sizes come from the library's autotuner
+    (d3q19_pool_autotune): advances of at least 100 steps time the candidate
+    grids of the pool's work class one by one, then keep the fastest."""
 
     def __init__(self, device: int = 0, storage: int = 0, rebuild_freq: int = 10, max_slots: int = 256,
-                 hbm_budget: int = 64 << 30, inplace: bool = False):
+                 hbm_budget: int = 64 << 30, inplace: bool = False, autotune: bool = True):
         self.lib = cuda_lib()
+        _tune_cache_load()
         h = C.c_void_p()
         rc = self.lib.d3q19_pool_create(device, storage, rebuild_freq, max_slots, hbm_budget, C.byref(h))
         if rc:
             raise D3Q19Error(f"d3q19_pool_create: {STATUS.get(rc, rc)}: {self.lib.d3q19_pool_last_error(None).decode()}")
         self.h = h
+        if autotune:
+            self._check(self.lib.d3q19_pool_autotune(self.h, 1), "pool_autotune")
         self.storage = storage
         self.inplace = int(inplace)  # members keep one distribution buffer (AA pattern)
         self.max_slots = max_slots
@@ -612,6 +676,29 @@ class Pool:
         self._check(self.lib.d3q19_pool_get_grid(self.h, C.byref(a), C.byref(b), C.byref(c)), "get_grid")
         return a.value, b.value, c.value
 
+    def autotune(self, enable: bool = True):
+        self._check(self.lib.d3q19_pool_autotune(self.h, int(enable)), "pool_autotune")
+
+    def tune_state(self) -> dict:
+        """The grid in use (CTAs per SM) and the tuner's progress on the
+        pool's current work class."""
+        v = [C.c_int() for _ in range(5)]
+        self._check(self.lib.d3q19_pool_tune_state(self.h, *[C.byref(x) for x in v]), "pool_tune_state")
+        return {"fluid_ctas_per_sm": v[0].value, "particle_ctas_per_sm": v[1].value, "settled": bool(v[2].value),
+                "tried": v[3].value, "candidates": v[4].value}
+
+    def tune_trials(self) -> list:
+        """[(fluid CTAs/SM, particle CTAs/SM, ns per fluid tile step or None)]
+        of the pool's current work class."""
+        n = C.c_int()
+        self._check(self.lib.d3q19_pool_tune_trials(self.h, None, None, None, 0, C.byref(n)), "pool_tune_trials")
+        f = np.zeros(n.value, np.int32)
+        q = np.zeros(n.value, np.int32)
+        t = np.zeros(n.value, np.float64)
+        self._check(self.lib.d3q19_pool_tune_trials(self.h, f.ctypes.data, q.ctypes.data, t.ctypes.data, n.value,
+                                                    C.byref(n)), "pool_tune_trials")
+        return [(int(a), int(b), float(c) if c >= 0 else None) for a, b, c in zip(f, q, t)]
+
     def synchronize(self):
         self._check(self.lib.d3q19_pool_synchronize(self.h), "pool_synchronize")
 
@@ -630,6 +717,7 @@ class Pool:
         if getattr(self, "h", None):
             self.lib.d3q19_pool_destroy(self.h)
             self.h = None
+            _tune_cache_save()
 
     def __del__(self):
         try:

@@ -423,9 +423,44 @@ int d3q19_pool_readmit(d3q19_pool* pool, const int_param_struct* ip, const flp_p
 /* Budget in use, the budget, and the member count. */
 int d3q19_pool_usage(d3q19_pool* pool, size_t* used, size_t* budget, int* members);
 /* Persistent grid sizes (CTAs) of the batched fluid, particle and contact
- * passes; the autotuner sets them.  Results do not depend on them. */
+ * passes.  Results do not depend on them.  d3q19_pool_set_grid turns the
+ * autotuner off. */
 int d3q19_pool_set_grid(d3q19_pool* pool, int fluid_blocks, int particle_blocks, int contact_blocks);
 int d3q19_pool_get_grid(d3q19_pool* pool, int* fluid_blocks, int* particle_blocks, int* contact_blocks);
+/* Grid autotuner (enable 1 on, 0 off; off when the pool is created).  With
+ * it on, d3q19_pool_advance takes the grid from a process-wide table keyed by
+ * the device (name and SM count), the pool's storage and layout, and the size
+ * class of its work (the bit length of its fluid tile count).  While the
+ * class has untried candidates -- fluid 2, 3, 4 CTAs per SM (also 5 for the
+ * two-buffer FP32 layout) by particle and contact 1, 2, 4 CTAs per SM -- an
+ * advance of at least 100 steps runs the next one and times it with events
+ * on the pool's stream; the next pool call collects the time, in ns per
+ * fluid tile step, and once every candidate has run the fastest becomes the
+ * class's choice, used by every later advance of that class on any pool of
+ * the process.  Results do not depend on the grid, so the timed advances are
+ * ordinary steps of the members. */
+int d3q19_pool_autotune(d3q19_pool* pool, int enable);
+/* The grid in use (CTAs per SM) and the tuner's state for the pool's current
+ * work class: settled (0/1), candidates timed, candidates in all.  Waits for
+ * a timed advance in flight. */
+int d3q19_pool_tune_state(d3q19_pool* pool, int* fluid_per_sm, int* particle_per_sm, int* settled, int* tried,
+                          int* total);
+/* The candidates of the current class with their times (ns per fluid tile
+ * step, negative when not yet timed): *n receives the candidate count; at
+ * most cap entries are written to each non-null array. */
+int d3q19_pool_tune_trials(d3q19_pool* pool, int* fluid_per_sm, int* particle_per_sm, double* ns_per_tile_step,
+                           int cap, int* n);
+/* The settled classes of the table as text, one line each, tab-separated:
+ * device name, SMs, storage, inplace, class, fluid CTAs per SM, particle CTAs
+ * per SM, ns per fluid tile step.  *len receives the text's length; the text
+ * and its NUL are written when cap exceeds it (else ENOMEM, or 0 for cap 0). */
+int d3q19_tune_export(char* buf, size_t cap, size_t* len);
+/* Adds settled classes in d3q19_tune_export's format (a later line of the
+ * same class replaces the earlier entry).  EINVAL, with nothing added, when
+ * a line does not parse. */
+int d3q19_tune_import(const char* text);
+/* Empties the table. */
+int d3q19_tune_clear(void);
 /* Without waiting: 1 when the work of the last d3q19_pool_advance has
  * finished on the device (or none was queued), 0 while it runs, negative on
  * a CUDA error.  For callers that run their own event loop. */

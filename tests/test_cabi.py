@@ -63,3 +63,40 @@ def test_invalid_parameters_rejected_before_device_use():
     assert rc == -1 and b"velocity boundaries" in lib.d3q19_last_error(None)
     cfg = d3.parse_config("total_lattice_size 8 8 8\nlattice_buffer_size 2 2 2\n")
     assert lib.d3q19_create(C.byref(cfg.ip), C.byref(cfg.fp), C.byref(d3.Options()), C.byref(h)) == -1
+
+
+def test_tuning_table_round_trip_without_gpu():
+    """The grid autotuner's table (d3q19_tune_import/export/clear) is host
+    state: lines in the export format come back unchanged; a malformed line
+    adds nothing."""
+    d3.tune_clear()
+    line = "NVIDIA B200\t148\t1\t0\t11\t3\t2\t412.5\n"
+    d3.tune_import(line)
+    assert d3.tune_export() == line
+    # A later line of the same class replaces the entry.
+    d3.tune_import(line.replace("\t3\t2\t412.5", "\t4\t1\t400"))
+    assert d3.tune_export() == line.replace("\t3\t2\t412.5", "\t4\t1\t400")
+    for bad in ("NVIDIA B200\t148\t1\t0\t11\t3\t2\n",          # a field missing
+                "NVIDIA B200\t148\t3\t0\t11\t3\t2\t1.0\n",      # storage out of range
+                "NVIDIA B200\t148\t1\t0\t11\t0\t2\t1.0\n",      # no CTAs
+                "NVIDIA B200\t148\t1\t0\t11\t3\t2\tfast\n",     # not a number
+                "\t148\t1\t0\t11\t3\t2\t1.0\n"):                # no device name
+        with pytest.raises(d3.D3Q19Error, match="EINVAL"):
+            d3.tune_import("H100\t132\t0\t0\t9\t2\t1\t5.0\n" + bad)
+    assert "H100" not in d3.tune_export()
+    d3.tune_clear()
+    assert d3.tune_export() == ""
+
+
+def test_tuning_cache_file(tmp_path, monkeypatch):
+    """D3Q19_TUNE_CACHE: the table is written to the file and read back."""
+    path = tmp_path / "tune.txt"
+    monkeypatch.setenv("D3Q19_TUNE_CACHE", str(path))
+    d3.tune_clear()
+    d3.tune_import("NVIDIA B200\t148\t0\t1\t12\t4\t2\t300\n")
+    d3._tune_cache_save()
+    d3.tune_clear()
+    monkeypatch.setattr(d3, "_TUNE_LOADED", False)
+    d3._tune_cache_load()
+    assert d3.tune_export() == path.read_text() == "NVIDIA B200\t148\t0\t1\t12\t4\t2\t300\n"
+    d3.tune_clear()
