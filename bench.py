@@ -662,7 +662,8 @@ def run_served(args):
     runs = {}
     for storage in (0, 1):
         pool = d3.Pool(storage=storage, max_slots=256, hbm_budget=100 << 30, inplace=args.inplace)
-        runs[storage] = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=max_steps).run(reqs)
+        runs[storage] = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=max_steps,
+                                  solo_nodes=args.solo_nodes or None).run(reqs)
         pool.close()
     # The autotuner's choices for the work classes the pools met (CTAs per SM
     # of the fluid and particle passes, ns per fluid tile step).
@@ -685,6 +686,9 @@ def run_served(args):
                        "edges": list(args.edges), "phi": [0.0, 0.3], "models": list(sv.MODELS),
                        "stop": "1e-4 over 500 steps",
                        "max_steps": max_steps, "pool_storage": "fp32",
+                       "solo_nodes": args.solo_nodes or None,
+                       "solo_requests": sum(1 for r in reqs if args.solo_nodes and
+                                            math.prod(e - 2 for e in r.edge) >= args.solo_nodes),
                        "pool_layout": "in place" if args.inplace else "two buffers"},
             "autotune": [{"storage": int(t[2]), "inplace": int(t[3]), "class_tiles": f"<2^{t[4]}",
                           "fluid_ctas_per_sm": int(t[5]), "particle_ctas_per_sm": int(t[6]),
@@ -841,6 +845,9 @@ def main():
     ap.add_argument("--edges", type=int, nargs=2, default=[32, 64], metavar=("LO", "HI"),
                     help="served-sweep: range of the cubic edges drawn")
     ap.add_argument("--max-steps", type=int, default=40000, help="served-sweep: step cap of a solve")
+    ap.add_argument("--solo-nodes", type=int, default=1 << 20,
+                    help="served-sweep: requests with at least this many interior nodes run on contexts of their "
+                         "own beside the pool (0: every request joins the pool)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fluid-kernel", default="tile", choices=sorted(FLUID_KERNELS),
                     help="collide-stream kernel: tile (the per-tile kernel) or tma (the TMA-pipelined kernel "

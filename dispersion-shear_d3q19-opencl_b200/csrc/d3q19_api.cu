@@ -1508,12 +1508,15 @@ struct d3q19_pool {
   long long steps = 0;
   // Grid autotuner (d3q19_pool_autotune): on or off, and the advance being
   // timed (its table key, candidate and fluid tile steps), if any.
+  struct TuneTrial {
+    std::string key;  // table entry
+    int cand;         // candidate timed
+    double units;     // fluid tile steps of the segment
+    cudaEvent_t e0, e1;
+  };
   bool tune = false;
-  bool tune_pending = false;
-  std::string tune_key;
-  int tune_cand = -1;
-  double tune_units = 0;
-  cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
+  std::vector<TuneTrial> tune_trials;                           // timed segments in flight
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tune_events;  // free event pairs
   char dev_name[256] = {0};
   // Every d3q19_pool_* call holds it: the pool may be driven from several
   // host threads (its members are not stepped outside these calls).
@@ -1582,7 +1585,6 @@ extern "C" int d3q19_pool_create(int device, int storage, int rebuild_freq, int 
   const unsigned long long keep = ~0ull;
   if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&p->ev_done, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreate(&p->ev_t0) != cudaSuccess || cudaEventCreate(&p->ev_t1) != cudaSuccess ||
       cudaMemPoolCreate(&p->mempool, &mp) != cudaSuccess ||
       cudaMemPoolSetAttribute(p->mempool, cudaMemPoolAttrReleaseThreshold, (void*)&keep) != cudaSuccess ||
       cudaMalloc(&p->d_fargs, sizeof(FluidArgs) * 2 * max_slots) != cudaSuccess ||
@@ -1812,51 +1814,114 @@ static TuneEntry tune_candidates(const d3q19_pool* p) {
   return e;
 }
 
-// Records the time of the timed advance in flight, if any (waits for it).
+// Records the times of the timed segments in flight (waits for them) and
+// settles the entries whose candidates have all been timed.
 static int tune_collect(d3q19_pool* p) {
-  if (!p->tune_pending) return 0;
-  p->tune_pending = false;
-  POOL_TRY(p, cudaEventSynchronize(p->ev_t1));
-  float ms = 0.f;
-  POOL_TRY(p, cudaEventElapsedTime(&ms, p->ev_t0, p->ev_t1));
-  std::lock_guard<std::mutex> lk(g_tune_mu);
-  auto it = g_tune.find(p->tune_key);
-  if (it == g_tune.end() || it->second.best >= 0 || p->tune_cand >= (int)it->second.cand.size()) return 0;
-  TuneEntry& e = it->second;
-  e.cost[p->tune_cand] = ms * 1e6 / p->tune_units;
-  int best = 0;
-  for (size_t i = 0; i < e.cost.size(); i++) {
-    if (e.cost[i] < 0) return 0;  // candidates left
-    if (e.cost[i] < e.cost[best]) best = (int)i;
+  if (p->tune_trials.empty()) return 0;
+  std::vector<std::pair<std::string, double>> got;
+  std::vector<int> cands;
+  cudaError_t err = cudaSuccess;
+  for (auto& t : p->tune_trials) {
+    float ms = 0.f;
+    cudaError_t e = cudaEventSynchronize(t.e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t.e0, t.e1);
+    if (e == cudaSuccess) {
+      got.emplace_back(t.key, ms * 1e6 / t.units);
+      cands.push_back(t.cand);
+    } else if (err == cudaSuccess) {
+      err = e;
+    }
+    p->tune_events.emplace_back(t.e0, t.e1);
   }
-  e.best = best;
-  // The choice applies from now on (the next advance of this class uses it).
-  p->fblocks = e.cand[best].first * p->sm_count;
-  p->pblocks = p->cblocks = e.cand[best].second * p->sm_count;
+  p->tune_trials.clear();
+  if (err != cudaSuccess) return pfail(p, D3Q19_ECUDA, "tuning events: %s", cudaGetErrorString(err));
+  const std::string cur =
+      tune_key_of(p->dev_name, p->sm_count, p->storage, p->inplace, tune_class(p->nf));
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (size_t i = 0; i < got.size(); i++) {
+    auto it = g_tune.find(got[i].first);
+    if (it == g_tune.end() || it->second.best >= 0 || cands[i] >= (int)it->second.cand.size()) continue;
+    TuneEntry& e = it->second;
+    e.cost[cands[i]] = got[i].second;
+    int best = 0;
+    bool all = true;
+    for (size_t j = 0; j < e.cost.size(); j++) {
+      all = all && e.cost[j] >= 0;
+      if (e.cost[j] >= 0 && (e.cost[best] < 0 || e.cost[j] < e.cost[best])) best = (int)j;
+    }
+    if (!all) continue;
+    e.best = best;
+    if (it->first == cur) {  // the choice applies from now on
+      p->fblocks = e.cand[best].first * p->sm_count;
+      p->pblocks = p->cblocks = e.cand[best].second * p->sm_count;
+    }
+  }
   return 0;
 }
 
-// Before an advance of nsteps: the grid of the pool's class, or the next
-// candidate to time.  Returns true when this advance is to be timed.
-static bool tune_choose(d3q19_pool* p, int nsteps) {
-  if (!p->tune || p->nf <= 0 || p->inplace < 0) return false;
+// Segment length of an advance of nsteps: while the pool's class has
+// candidates left, an advance of at least two segments is run as segments of
+// TUNE_MIN_STEPS (rounded up to the period), each timing one candidate.
+static int tune_segment(const d3q19_pool* p, int nsteps) {
+  if (!p->tune || p->nf <= 0 || p->inplace < 0) return nsteps;
+  const int seg = (TUNE_MIN_STEPS + p->period - 1) / p->period * p->period;
+  if (nsteps < 2 * seg) return nsteps;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_key_of(p->dev_name, p->sm_count, p->storage, p->inplace, tune_class(p->nf)));
+  return it != g_tune.end() && it->second.best >= 0 ? nsteps : seg;
+}
+
+// Before a segment of nsteps: sets the grid of the pool's class -- its
+// choice, else the next candidate not yet timed nor in flight, else the
+// fastest timed so far.  Returns the candidate to time, or -1.
+static int tune_choose(d3q19_pool* p, int nsteps, std::string* key_out) {
+  if (!p->tune || p->nf <= 0 || p->inplace < 0) return -1;
   const std::string key = tune_key_of(p->dev_name, p->sm_count, p->storage, p->inplace, tune_class(p->nf));
   std::lock_guard<std::mutex> lk(g_tune_mu);
   auto it = g_tune.find(key);
   if (it == g_tune.end()) it = g_tune.emplace(key, tune_candidates(p)).first;
   const TuneEntry& e = it->second;
-  int c = e.best;
-  if (c < 0 && nsteps >= TUNE_MIN_STEPS)
-    for (c = 0; c < (int)e.cost.size() && e.cost[c] >= 0; c++) {
+  int c = e.best, timed = -1;
+  if (c < 0 && nsteps >= TUNE_MIN_STEPS) {
+    for (int i = 0; i < (int)e.cost.size() && timed < 0; i++) {
+      if (e.cost[i] >= 0) continue;
+      bool busy = false;
+      for (const auto& t : p->tune_trials) busy = busy || (t.cand == i && t.key == key);
+      if (!busy) timed = i;
     }
-  if (c < 0 || c >= (int)e.cand.size()) return false;
+    c = timed;
+  }
+  if (c < 0)
+    for (int i = 0; i < (int)e.cost.size(); i++)
+      if (e.cost[i] >= 0 && (c < 0 || e.cost[i] < e.cost[c])) c = i;
+  if (c < 0) return -1;
   p->fblocks = e.cand[c].first * p->sm_count;
   p->pblocks = p->cblocks = e.cand[c].second * p->sm_count;
-  if (e.best >= 0) return false;
-  p->tune_key = key;
-  p->tune_cand = c;
-  p->tune_units = (double)nsteps * (double)p->nf;
-  return true;
+  if (timed >= 0) *key_out = key;
+  return timed;
+}
+
+// The graph of a chunk of nsteps at the pool's current grid (captured on
+// first use).
+static int pool_graph(d3q19_pool* p, int nsteps, cudaGraphExec_t* out) {
+  auto key = std::make_tuple(nsteps, p->fblocks, p->pblocks, p->cblocks, p->inplace);
+  auto it = p->graphs.find(key);
+  if (it == p->graphs.end()) {
+    cudaGraph_t graph;
+    POOL_TRY(p, cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = pool_enqueue(p, nsteps);
+    cudaError_t e = cudaStreamEndCapture(p->stream, &graph);
+    if (rc) return rc;
+    if (e != cudaSuccess) return pfail(p, D3Q19_ECUDA, "pool capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return pfail(p, D3Q19_ECUDA, "pool graph: %s", cudaGetErrorString(e));
+    it = p->graphs.emplace(key, exec).first;
+    POOL_TRY(p, cudaGraphUpload(exec, p->stream));  // not inside a timed segment
+  }
+  *out = it->second;
+  return 0;
 }
 
 extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
@@ -1875,28 +1940,34 @@ extern "C" int d3q19_pool_advance(d3q19_pool* p, int nsteps) {
   if (int rc = tune_collect(p)) return rc;
   if (p->dirty)
     if (int rc = pool_upload(p)) return rc;
-  const bool timed = tune_choose(p, nsteps);
-  auto key = std::make_tuple(nsteps, p->fblocks, p->pblocks, p->cblocks, p->inplace);
-  auto it = p->graphs.find(key);
-  if (it == p->graphs.end()) {
-    cudaGraph_t graph;
-    POOL_TRY(p, cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = pool_enqueue(p, nsteps);
-    cudaError_t e = cudaStreamEndCapture(p->stream, &graph);
-    if (rc) return rc;
-    if (e != cudaSuccess) return pfail(p, D3Q19_ECUDA, "pool capture: %s", cudaGetErrorString(e));
+  const int seg = tune_segment(p, nsteps);
+  for (int done = 0; done < nsteps;) {
+    std::string tkey;
+    int len = std::min(seg, nsteps - done);
+    const int cand = tune_choose(p, len, &tkey);
+    if (cand < 0) len = nsteps - done;  // nothing to time: the rest in one graph
     cudaGraphExec_t exec;
-    e = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) return pfail(p, D3Q19_ECUDA, "pool graph: %s", cudaGetErrorString(e));
-    it = p->graphs.emplace(key, exec).first;
-    POOL_TRY(p, cudaGraphUpload(exec, p->stream));  // not inside a timed advance
-  }
-  if (timed) POOL_TRY(p, cudaEventRecord(p->ev_t0, p->stream));
-  POOL_TRY(p, cudaGraphLaunch(it->second, p->stream));
-  if (timed) {
-    POOL_TRY(p, cudaEventRecord(p->ev_t1, p->stream));
-    p->tune_pending = true;
+    if (int rc = pool_graph(p, len, &exec)) return rc;
+    if (cand >= 0) {
+      if (p->tune_events.empty()) {
+        cudaEvent_t e0, e1;
+        POOL_TRY(p, cudaEventCreate(&e0));
+        if (cudaEventCreate(&e1) != cudaSuccess) {
+          cudaEventDestroy(e0);
+          return pfail(p, D3Q19_ECUDA, "tuning events");
+        }
+        p->tune_events.emplace_back(e0, e1);
+      }
+      const auto ev = p->tune_events.back();
+      p->tune_events.pop_back();
+      p->tune_trials.push_back({tkey, cand, (double)len * (double)p->nf, ev.first, ev.second});
+      POOL_TRY(p, cudaEventRecord(ev.first, p->stream));
+      POOL_TRY(p, cudaGraphLaunch(exec, p->stream));
+      POOL_TRY(p, cudaEventRecord(ev.second, p->stream));
+    } else {
+      POOL_TRY(p, cudaGraphLaunch(exec, p->stream));
+    }
+    done += len;
   }
   POOL_TRY(p, cudaEventRecord(p->ev_done, p->stream));
   for (int s = 0; s < p->max_slots; s++) {
@@ -2256,8 +2327,10 @@ extern "C" int d3q19_pool_destroy(d3q19_pool* p) {
   if (p->stream) cudaStreamSynchronize(p->stream);  // the members' stream-ordered frees
   if (p->mempool) cudaMemPoolDestroy(p->mempool);
   if (p->ev_done) cudaEventDestroy(p->ev_done);
-  if (p->ev_t0) cudaEventDestroy(p->ev_t0);
-  if (p->ev_t1) cudaEventDestroy(p->ev_t1);
+  for (auto& e : p->tune_events) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
   return 0;

@@ -557,6 +557,7 @@ class Pool:
         if rc:
             raise D3Q19Error(f"d3q19_pool_create: {STATUS.get(rc, rc)}: {self.lib.d3q19_pool_last_error(None).decode()}")
         self.h = h
+        self.device = device
         if autotune:
             self._check(self.lib.d3q19_pool_autotune(self.h, 1), "pool_autotune")
         self.storage = storage

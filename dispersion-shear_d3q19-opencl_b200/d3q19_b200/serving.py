@@ -179,14 +179,35 @@ class Server:
 
     cancel(rid), from any thread, stops a request at the next chunk
     boundary: a queued one is never admitted, a running one is released, a
-    parked one drops its checkpoint; its record has cancelled = True."""
+    parked one drops its checkpoint; its record has cancelled = True.
+
+    solo_nodes: None (off) or an interior node count.  A request at least
+    that large runs on a context of its own (the single-lattice kernels,
+    faster per node than the batched ones, and a large lattice fills the GPU
+    alone) instead of a pool slot, concurrently with the pool on its own
+    stream, with the same stop rule; at most solo_slots of them at a time,
+    within solo_budget bytes of device memory.  Admission stays in arrival
+    order: a solo request that does not fit waits at the head of the queue.
+    make_solo(hs) and solo_bytes(hs) create such a context and give its
+    device bytes (by default a Simulation with the pool's storage and
+    layout, and d3q19_context_bytes)."""
 
     def __init__(self, pool: Pool, check_every: int = 500, rel_tol: float = 1e-4, max_steps: int = 20000,
-                 clock=time.perf_counter, sleep=time.sleep, builders: int = 4, preempt_after: int | None = None):
+                 clock=time.perf_counter, sleep=time.sleep, builders: int = 4, preempt_after: int | None = None,
+                 solo_nodes: int | None = None, solo_slots: int = 2, solo_budget: int = 32 << 30,
+                 make_solo=None, solo_bytes=None):
         if check_every % pool.period:
             raise ValueError(f"check_every must be a multiple of the pool period {pool.period}")
         if preempt_after is not None and preempt_after <= 0:
             raise ValueError("preempt_after must be positive")
+        if solo_nodes is not None and (solo_nodes <= 0 or solo_slots <= 0):
+            raise ValueError("solo_nodes and solo_slots must be positive")
+        self.solo_nodes = solo_nodes
+        self.solo_slots = solo_slots
+        self.solo_budget = solo_budget
+        self.make_solo = make_solo or (lambda hs: Simulation.from_host_state(
+            hs, device=pool.device, storage=pool.storage, inplace=pool.inplace))
+        self.solo_bytes = solo_bytes or (lambda hs: _solo_context_bytes(hs, pool))
         self.pool = pool
         self.check_every = check_every
         self.rel_tol = rel_tol
@@ -234,7 +255,14 @@ class Server:
         done = []
         ex = ThreadPoolExecutor(max_workers=self.builders) if self.builders > 0 else None
         built = {}  # rid -> Future or host state of an arrived request
+        solo = {}   # rid -> _Solo: requests on contexts of their own
         qi = nb = 0
+
+        def is_solo(req):
+            return self.solo_nodes is not None and math.prod(e - 2 for e in req.edge) >= self.solo_nodes
+
+        def solo_used():
+            return sum(so.bytes for so in solo.values())
 
         def prepare():
             # Start the set-up of every request that has arrived.
@@ -270,6 +298,8 @@ class Server:
             if self.preempt_after is None or qi >= nb or (parked and parked[0][0] <= qi):
                 return
             req = queue[qi]
+            if is_solo(req):  # not a pool member: evictions would not make room for it
+                return
             hs = built[req.rid]
             if ex:
                 hs = hs.result()
@@ -299,10 +329,22 @@ class Server:
                 hs = built[req.rid]
                 if ex:
                     hs = hs.result()
+                if is_solo(req):
+                    nbytes = self.solo_bytes(hs)
+                    if len(solo) >= self.solo_slots or solo_used() + nbytes > self.solo_budget:
+                        built[req.rid] = hs if not ex else _done_future(hs)
+                        if not solo and nbytes > self.solo_budget:
+                            raise RuntimeError(f"request {req.rid} does not fit the solo budget")
+                        return
+                    del built[req.rid]
+                    solo[req.rid] = _Solo(_Member(req, self.clock() - t0, Convergence(self.rel_tol)),
+                                          self.make_solo(hs), nbytes)
+                    qi += 1
+                    continue
                 slot = self.pool.admit(hs)
                 if slot is None:
                     built[req.rid] = hs if not ex else _done_future(hs)
-                    if not active and not joining:
+                    if not active and not joining and not solo:
                         raise RuntimeError(f"request {req.rid} does not fit an empty pool")
                     return
                 del built[req.rid]
@@ -322,6 +364,11 @@ class Server:
                     done.append(SolveRecord(m.req.rid, m.req.arrival, m.start, now, self.pool.steps(slot),
                                             float("nan"), float("nan"), False, False, m.preempted, True))
                     self.pool.release(slot)
+            for rid in [r for r in solo if r in gone]:
+                so = solo.pop(rid)
+                done.append(SolveRecord(rid, so.m.req.arrival, so.m.start, now, so.t - 1, float("nan"),
+                                        float("nan"), False, False, 0, True))
+                so.sim.close()
             for entry in [e for e in parked if e[1].req.rid in gone]:
                 parked.remove(entry)
                 m = entry[1]
@@ -343,29 +390,50 @@ class Server:
                 self._cancel -= gone
 
         try:
-            while qi < len(queue) or active or joining or parked:
+            while qi < len(queue) or active or joining or parked or solo:
                 cancel_requested()
-                if not (qi < len(queue) or active or joining or parked):
+                if not (qi < len(queue) or active or joining or parked or solo):
                     break
                 # Between chunks the GPU waits for the host, so requests are
                 # admitted here only into an empty pool; otherwise they are
                 # admitted while the next chunk runs.  Evictions need the
                 # members' state at a chunk boundary: they happen here.
-                if active or joining:
+                if active or joining or solo:
                     make_room()
                 else:
                     admit_arrived()
                 active.update(joining)
                 joining.clear()
-                if not active:
+                if not active and not solo:
                     if qi < len(queue):
                         self.sleep(max(0.0, queue[qi].arrival - (self.clock() - t0)))
                     continue
-                # The chunk runs on the pool's stream while the host admits the
-                # requests that arrived meanwhile (their set-up and first steps
-                # overlap the chunk on the device); they join the next chunk.
-                self.pool.advance(self.check_every)
+                # The chunk runs on the pool's stream (and the solo contexts'
+                # chunks on theirs) while the host admits the requests that
+                # arrived meanwhile (their set-up and first steps overlap the
+                # chunk on the device); they join the next chunk.
+                for so in solo.values():
+                    so.sim.run(so.t, self.check_every)
+                    so.t += self.check_every
+                if active:
+                    self.pool.advance(self.check_every)
                 admit_arrived()
+                for rid in list(solo):
+                    so = solo[rid]
+                    try:
+                        stress, _, visc = so.sim.mean_stress()
+                        failed = False
+                    except D3Q19Error:
+                        stress = visc = float("nan")
+                        failed = True
+                    ok = not failed and so.m.conv.update(stress)
+                    if failed or ok or so.t - 1 >= self.max_steps:
+                        done.append(SolveRecord(rid, so.m.req.arrival, so.m.start, self.clock() - t0, so.t - 1,
+                                                stress, visc, ok, failed))
+                        so.sim.close()
+                        del solo[rid]
+                if not active:
+                    continue
                 stresses = self._stresses(active)
                 for slot in list(active):
                     m = active[slot]
@@ -391,6 +459,23 @@ class Server:
             if ex:
                 ex.shutdown(wait=True)
         return done, self.clock() - t0
+
+
+@dataclasses.dataclass
+class _Solo:
+    m: _Member
+    sim: object
+    bytes: int
+    t: int = 1  # next step
+
+
+def _solo_context_bytes(hs, pool) -> int:
+    from . import context_bytes
+
+    opt = Options.from_buffer_copy(bytes(hs.options))
+    opt.storage = pool.storage
+    opt.inplace = pool.inplace
+    return context_bytes(hs.cfg.ip, opt)
 
 
 def _done_future(value):

@@ -433,11 +433,14 @@ int d3q19_pool_get_grid(d3q19_pool* pool, int* fluid_blocks, int* particle_block
  * class of its work (the bit length of its fluid tile count).  While the
  * class has untried candidates -- fluid 2, 3, 4 CTAs per SM (also 5 for the
  * two-buffer FP32 layout) by particle and contact 1, 2, 4 CTAs per SM -- an
- * advance of at least 100 steps runs the next one and times it with events
- * on the pool's stream; the next pool call collects the time, in ns per
- * fluid tile step, and once every candidate has run the fastest becomes the
- * class's choice, used by every later advance of that class on any pool of
- * the process.  Results do not depend on the grid, so the timed advances are
+ * advance runs them in segments of 100 steps (rounded up to the period; an
+ * advance shorter than two segments is one segment, timed when it has at
+ * least 100 steps), one candidate per segment, each timed with events on the
+ * pool's stream; the rest of the advance runs at the fastest grid timed so
+ * far.  The next pool call collects the times, in ns per fluid tile step,
+ * and once every candidate has been timed the fastest becomes the class's
+ * choice, used by every later advance of that class on any pool of the
+ * process.  Results do not depend on the grid, so the timed segments are
  * ordinary steps of the members. */
 int d3q19_pool_autotune(d3q19_pool* pool, int enable);
 /* The grid in use (CTAs per SM) and the tuner's state for the pool's current

@@ -4,7 +4,8 @@
   class one by one; once all have run, the fastest is kept and used.
 * The tuning changes no result: the members end bit for bit where a pool
   with a fixed grid leaves them.
-* Shorter advances are not timed.
+* Shorter advances are not timed; a long advance times one candidate per
+  100-step segment.
 * The table exported by one process seeds another: an imported class is
   settled at once.
 """
@@ -73,3 +74,23 @@ def test_imported_class_is_settled_at_once():
         (choice["fluid_ctas_per_sm"], choice["particle_ctas_per_sm"])
     pool.close()
     d3.tune_clear()
+
+
+def test_long_advance_times_one_candidate_per_segment():
+    d3.tune_clear()
+    pool, slots = pool_with(REQS[:2], True)
+    pool.advance(500)  # five segments of 100 steps, five candidates
+    st = pool.tune_state()
+    assert st["tried"] == 5 and not st["settled"]
+    pool.advance(500)  # the other four, then the fastest so far
+    st = pool.tune_state()
+    assert st["settled"] and st["tried"] == st["candidates"] == 9
+    best = min(pool.tune_trials(), key=lambda x: x[2])
+    assert (st["fluid_ctas_per_sm"], st["particle_ctas_per_sm"]) == best[:2]
+    tuned = [state(pool, s) for s in slots]
+    pool.close()
+    fixed, slots = pool_with(REQS[:2], False)
+    fixed.advance(1000)
+    for s, t in zip(slots, tuned):
+        bits_equal(t, state(fixed, s))
+    fixed.close()

@@ -283,3 +283,47 @@ def test_cancel_queued_running_and_parked():
     assert all(by[k].converged and not by[k].cancelled for k in (2, 3))
     assert pool.used == 0 and sv.summary(recs, 1.0)["cancelled"] == sum(r.cancelled for r in recs)
     assert 1 in pool.evicted and by[1].cancelled and 1 not in pool.readmitted
+
+
+class FakeSolo:
+    live = 0
+    peak = 0
+
+    def __init__(self, hs):
+        self.hs, self.steps = hs, 0
+        FakeSolo.live += 1
+        FakeSolo.peak = max(FakeSolo.peak, FakeSolo.live)
+
+    def run(self, t0, n):
+        assert t0 == self.steps + 1
+        self.steps += n
+
+    def mean_stress(self):
+        return self.hs["target"] * (1.0 - np.exp(-self.steps / 1000.0)), 0.0, 0.0
+
+    def close(self):
+        FakeSolo.live -= 1
+
+
+def test_large_requests_run_on_contexts_of_their_own():
+    """solo_nodes: requests at least that large bypass the pool and run on
+    their own contexts (at most solo_slots at a time, within solo_budget),
+    in arrival order, with the same stop rule; the small ones share the
+    pool meanwhile."""
+    edges = [32, 160, 40, 150, 36, 140, 34, 130]
+    reqs = [sv.ShearRequest(rid=i, edge=(e, e, e), phi=0.0, model="newtonian", wall_speed=0.02, seed=1,
+                            arrival=0.0) for i, e in enumerate(edges)]
+    pool = FakePool(budget=100)
+    FakeSolo.live = FakeSolo.peak = 0
+    build = lambda r: {"bytes": 10, "rid": r.rid, "target": 1.0 + r.rid, "edge": r.edge[0]}
+    srv = sv.Server(pool, check_every=500, rel_tol=1e-4, max_steps=30000, clock=lambda: 0.0,
+                    sleep=lambda dt: None, solo_nodes=100 ** 3, solo_slots=2, solo_budget=25,
+                    make_solo=FakeSolo, solo_bytes=lambda hs: 10)
+    recs, _ = srv.run(reqs, build=build)
+    assert sorted(r.rid for r in recs) == list(range(8))
+    assert pool.admitted == [0, 2, 4, 6]          # the small ones only
+    assert FakeSolo.peak == 2 and FakeSolo.live == 0
+    assert all(r.converged and r.steps % 500 == 0 for r in recs if r.rid % 2)
+    assert all(r.converged for r in recs)
+    with pytest.raises(ValueError):
+        sv.Server(pool, solo_nodes=0)
