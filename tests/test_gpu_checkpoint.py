@@ -194,7 +194,8 @@ def _ckpt_layout(ck):
     return out, dict(np=npar, Z=Z, cap=cap, ntiles=ntiles)
 
 
-@pytest.mark.parametrize("damage", ["zone_member", "tile_list", "reverse_table", "neighbour_count"])
+@pytest.mark.parametrize("damage", ["zone_member", "tile_list", "reverse_table", "neighbour_count", "neighbour_id",
+                                    "pars_zone", "zone_of"])
 def test_restore_refuses_damaged_tables(damage):
     # A checkpoint's integer tables index device arrays: a damaged entry is
     # refused on the host before anything is uploaded.
@@ -217,11 +218,41 @@ def test_restore_refuses_damaged_tables(damage):
         view("tile_list", dims["ntiles"] * dims["cap"])[T * dims["cap"]] = -3
     elif damage == "reverse_table":
         view("revStart", dims["Z"] + 1)[dims["Z"]] = 27 * dims["Z"] + 5
-    else:
+    elif damage == "neighbour_count":
         view("znd", 28 * dims["Z"])[0] = 99
+    elif damage == "neighbour_id":
+        znd = ints("znd", 28 * dims["Z"])
+        assert znd[0] > 0
+        view("znd", 28 * dims["Z"])[1] = dims["Z"] + 2
+    elif damage == "pars_zone":
+        view("parsZone", dims["np"])[0] = dims["Z"] + 3
+    else:
+        view("zoneOf", dims["np"])[0] = -1
     with pytest.raises(d3.D3Q19Error, match="damaged"):
         a.restore(bad)
     a.restore(ck)  # the intact one still restores
     a.run(11, 5)
+    a.synchronize()
+    a.close()
+
+
+@pytest.mark.parametrize("field,value", [("phase", 5), ("f_state", 7), ("last_t", -4)])
+def test_restore_refuses_damaged_header(field, value):
+    # The header's layout phase, distribution state and step are checked
+    # before anything is uploaded (an in-place context: the phase selects
+    # its buffer).
+    import struct
+
+    hs = sv.host_state(SUSP)
+    a = d3.Simulation.from_host_state(hs, inplace=1)
+    a.run(1, 11)
+    ck = a.checkpoint()
+    off = {"f_state": 60, "last_t": 64, "phase": 76}[field]
+    bad = ck.copy()
+    bad[off:off + 4] = np.frombuffer(struct.pack("<i", value), np.uint8)
+    with pytest.raises(d3.D3Q19Error):
+        a.restore(bad)
+    a.restore(ck)
+    a.run(12, 5)
     a.synchronize()
     a.close()
