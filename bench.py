@@ -343,27 +343,29 @@ def run_ours(args, rank, world, local_rank, dist):
 
     hf, hu, htau = pinned(hs.f), pinned(hs.u), pinned(hs.tau)
     hk, hpf, hpff, hsp = pinned(hs.parKin), pinned(hs.parForce), pinned(hs.parFluidForce), pinned(hs.spherePoints)
-    ru, rk, rpff = pinned(np.zeros(3 * sim.nc, np.float32)), pinned(np.zeros(max(hs.parKin.size, 1), np.float32)), \
-        pinned(np.zeros(max(hs.parFluidForce.size, 1), np.float32))
+    ru = pinned(np.zeros(3 * sim.nc, np.float32))
+    rk = pinned(np.zeros(16 * sim.np, np.float32))
+    rpff = pinned(np.zeros(8 * sim.np * sim.nfa, np.float32))
+    hpm = pinned(d3.periodic_map(hs.cfg.ip))  # an input array, prepared on the host like the others
     sim2 = d3.Simulation(hs.cfg.ip, hs.cfg.fp, hs.options)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     w0 = time.perf_counter()
     sim2.write_lattice(hf, hu, htau)
-    sim2.write_periodic_map(d3.periodic_map(hs.cfg.ip))
+    sim2.write_periodic_map(hpm)
     if sim2.np > 0:
         sim2.write_particles(hk, hpf, hpff, hsp)
         sim2.write_zones(hs.zoneNeighDat, hs.parsZone, hs.zoneMembers, hs.numParInZone, hs.threadMembers,
                          hs.numParInThread)
     sim2.run(1, args.steps)
-    ru[:] = sim2.read_u()
+    sim2.read_u(out=ru)  # straight into pinned host memory
     if sim2.np > 0:
-        rk[:] = sim2.read_parkin()
-        rpff[:] = sim2.read_parfluidforce()
+        sim2.read_parkin(out=rk)
+        sim2.read_parfluidforce(out=rpff)
     e2e_s = time.perf_counter() - w0
     e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{local_rank}")
-    h2d = hf.nbytes + hu.nbytes + htau.nbytes + hk.nbytes + hpf.nbytes + hpff.nbytes + hsp.nbytes
+    h2d = hf.nbytes + hu.nbytes + htau.nbytes + hpm.nbytes + hk.nbytes + hpf.nbytes + hpff.nbytes + hsp.nbytes
     d2h = ru.nbytes + (rk.nbytes + rpff.nbytes if sim2.np > 0 else 0)
     sim2.close()
     sim.close()

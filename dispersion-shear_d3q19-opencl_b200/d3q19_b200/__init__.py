@@ -365,13 +365,18 @@ class Simulation:
     def synchronize(self):
         self._check(self.lib.d3q19_synchronize(self.h), "synchronize")
 
-    def _read(self, fn, n, dtype=np.float32):
-        out = np.zeros(n, dtype)
+    def _read(self, fn, n, dtype=np.float32, out=None):
+        """out: an existing C-contiguous array of n elements of dtype to read
+        into (for example pinned host memory), else a new one."""
+        if out is None:
+            out = np.zeros(n, dtype)
+        elif out.dtype != dtype or out.size != n or not out.flags.c_contiguous:
+            raise ValueError(f"{fn}: out must be a contiguous {dtype.__name__} array of {n} elements")
         self._check(getattr(self.lib, fn)(self.h, _ptr(out)), fn)
         return out
 
-    def read_u(self):
-        return self._read("d3q19_read_u", 3 * self.nc)
+    def read_u(self, out=None):
+        return self._read("d3q19_read_u", 3 * self.nc, out=out)
 
     def read_tau(self):
         return self._read("d3q19_read_tau", self.nc)
@@ -379,8 +384,8 @@ class Simulation:
     def read_f(self):
         return self._read("d3q19_read_f", 19 * self.nc)
 
-    def read_parkin(self):
-        return self._read("d3q19_read_parkin", 16 * self.np)
+    def read_parkin(self, out=None):
+        return self._read("d3q19_read_parkin", 16 * self.np, out=out)
 
     def read_parkin64(self):
         """The FP64 sphere state (particle_precision = 1 or the FP64 build)."""
@@ -389,8 +394,8 @@ class Simulation:
     def read_parforce(self):
         return self._read("d3q19_read_parforce", 8 * self.np)
 
-    def read_parfluidforce(self):
-        return self._read("d3q19_read_parfluidforce", 8 * self.np * self.nfa)
+    def read_parfluidforce(self, out=None):
+        return self._read("d3q19_read_parfluidforce", 8 * self.np * self.nfa, out=out)
 
     def read_spread_force(self):
         return self._read("d3q19_read_spread_force", 3 * self.nc)

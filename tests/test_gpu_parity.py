@@ -211,5 +211,14 @@ def test_prepared_short_run_matches_eager_steps():
     for rd in ("read_u", "read_f", "read_parkin", "read_parfluidforce", "read_parforce"):
         x, y = getattr(a, rd)(), getattr(b, rd)()
         assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), rd
+    # Read-backs into a caller's buffer give the same bytes; a buffer of the
+    # wrong size is refused before the call.
+    for rd in ("read_u", "read_parkin", "read_parfluidforce"):
+        ref = getattr(a, rd)()
+        buf = np.full(ref.size, np.nan, np.float32)
+        assert getattr(a, rd)(out=buf) is buf
+        assert np.array_equal(buf.view(np.uint32), ref.view(np.uint32)), rd
+        with pytest.raises(ValueError):
+            getattr(a, rd)(out=np.zeros(ref.size + 1, np.float32))
     a.close()
     b.close()
