@@ -629,6 +629,38 @@ def run_batch(args):
             "speedup_vs_one_at_a_time_fp32": round(batched / alone, 2)}
 
 
+def run_pool_mix(args):
+    """cfg: the served sweep's first 48 requests resident in one FP32
+    in-place pool at the default grid (no autotuner), advanced together: the
+    batched kernels on a served mix, for profiling."""
+    import torch
+
+    import d3q19_b200 as d3
+    from d3q19_b200 import serving as sv
+
+    torch.cuda.set_device(0)
+    reqs = sv.make_requests(48, 50.0, 2024, edges=(32, 64))
+    pool = d3.Pool(storage=0, max_slots=64, hbm_budget=40 << 30, inplace=True, autotune=False)
+    for r in reqs:
+        if pool.admit(sv.host_state(r)) is None:
+            raise RuntimeError("the mix does not fit the pool")
+    nodes = sum((r.edge[0] - 2) ** 3 for r in reqs)
+    tiles = sum(math.ceil((r.edge[0] - 2) / 32) * math.ceil((r.edge[0] - 2) / 4) ** 2 for r in reqs)
+    period = pool.period
+    pool.advance(max(period, args.warmup // period * period))  # capture and warm-up
+    steps = max(period, args.steps // period * period)
+    pool.advance(steps)  # capture of the timed chunk length
+    ms = _time_pool(pool, steps, pool.stream_ptr, torch)
+    pool.close()
+    return {"metric": "MLUPS (served mix in one pool)", "value": round(nodes * steps / (ms * 1e-3) / 1e6, 1),
+            "unit": "MLUPS", "n_gpus": 1, "steps": steps, "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic (seeded)", "impl": "ours",
+            "config": {"workload": "pool-mix", "requests": len(reqs), "interior_nodes": nodes, "tiles": tiles,
+                       "description": "the served sweep's first 48 requests (edges 32-64, phi 0-0.3, three laws) "
+                                      "in one FP32 in-place pool, default grid"},
+            "ns_per_tile_step": round(ms * 1e6 / (steps * tiles), 2)}
+
+
 def warm_served_paths(storages, alone=True):
     """Untimed: a short burst through a pool of each storage (and, with
     alone, one solve on its own context), so that the timed runs do not pay
@@ -842,7 +874,8 @@ def main():
     ap.add_argument("--workload", default="suspension-128", choices=sorted(WORKLOADS) + ["batch-64",
                                                                                            "served-sweep",
                                                                                            "served-preempt",
-                                                                                           "casson-precision"])
+                                                                                           "casson-precision",
+                                                                                           "pool-mix"])
     ap.add_argument("--requests", type=int, default=128, help="served-sweep: number of requests")
     ap.add_argument("--edges", type=int, nargs=2, default=[32, 64], metavar=("LO", "HI"),
                     help="served-sweep: range of the cubic edges drawn")
@@ -870,10 +903,10 @@ def main():
         if rank == 0:
             print(json.dumps(run_reference_arm(args)), flush=True)
         return
-    if args.workload in ("batch-64", "served-sweep", "served-preempt", "casson-precision"):
+    if args.workload in ("batch-64", "served-sweep", "served-preempt", "casson-precision", "pool-mix"):
         if rank == 0:
             run = {"batch-64": run_batch, "served-sweep": run_served, "served-preempt": run_served_preempt,
-                   "casson-precision": run_precision}
+                   "casson-precision": run_precision, "pool-mix": run_pool_mix}
             print(json.dumps(run[args.workload](args)), flush=True)
         return
     dist = None
