@@ -581,9 +581,10 @@ def run_batch(args):
         if pool.admit(hs) is None:
             raise RuntimeError("batch does not fit the pool")
     # The library's grid autotuner (d3q19_pool_autotune): each 200-step
-    # advance of the live batch times the next candidate grid of the batch's
-    # work class until every candidate has run; the fastest is kept.  The
-    # results do not depend on the grid, so these are ordinary steps.
+    # advance of the live batch times the next candidate particle/contact
+    # grid of the batch's work class until every candidate has run; the
+    # fastest is kept (the fluid pass runs one CTA per tile).  The results do
+    # not depend on the grid, so these are ordinary steps.
     d3.tune_clear()
     tuning_steps = 0
     while not pool.tune_state()["settled"]:
@@ -620,10 +621,10 @@ def run_batch(args):
             "config": {"workload": "batch-64", "boxes": len(states), "interior_nodes": nodes,
                        "description": "64 boxes, edges from {32,48,64,96} per axis, 1-20 spheres of radius 4-8, "
                                       "power-law n in [0.4,1], walls +-[0.01,0.05]; one launch per pass for all"},
-            "autotune": {"fluid_ctas_per_sm": best[0], "particle_ctas_per_sm": best[1],
-                         "grid_in_use": [g // sms for g in grid], "tuning_steps": tuning_steps,
-                         "default_grid": [4, 4],
-                         "trials_ns_per_tile_step": [[f, pp, round(t, 2)] for f, pp, t in trials],
+            "autotune": {"particle_ctas_per_sm": best[1], "particle_ctas_per_sm_in_use": grid[1] // sms,
+                         "fluid_grid": grid[0], "fluid": "one CTA per tile", "tuning_steps": tuning_steps,
+                         "default_particle_ctas_per_sm": 4,
+                         "trials_ns_per_tile_step": [[pp, round(t, 2)] for _, pp, t in trials],
                          "tile": "32x4x4"},
             "one_at_a_time_fp32": {"value": round(alone, 1), "unit": "MLUPS"},
             "speedup_vs_one_at_a_time_fp32": round(batched / alone, 2)}
@@ -631,8 +632,8 @@ def run_batch(args):
 
 def run_pool_mix(args):
     """cfg: the served sweep's first 48 requests resident in one FP32
-    in-place pool at the default grid (no autotuner), advanced together: the
-    batched kernels on a served mix, for profiling."""
+    in-place pool at the default particle grid (no autotuner), advanced
+    together: the batched kernels on a served mix, for profiling."""
     import torch
 
     import d3q19_b200 as d3
@@ -645,7 +646,8 @@ def run_pool_mix(args):
         if pool.admit(sv.host_state(r)) is None:
             raise RuntimeError("the mix does not fit the pool")
     nodes = sum((r.edge[0] - 2) ** 3 for r in reqs)
-    tiles = sum(math.ceil((r.edge[0] - 2) / 32) * math.ceil((r.edge[0] - 2) / 4) ** 2 for r in reqs)
+    # 32 x 4 x 4 tiles from the lattice origin, buffer layers included (as the kernels tile)
+    tiles = sum(math.ceil(r.edge[0] / 32) * math.ceil(r.edge[1] / 4) * math.ceil(r.edge[2] / 4) for r in reqs)
     period = pool.period
     pool.advance(max(period, args.warmup // period * period))  # capture and warm-up
     steps = max(period, args.steps // period * period)

@@ -1496,7 +1496,8 @@ struct d3q19_pool {
   long long nf = 0, ngr = 0, nsph = 0;  // item counts of the current lists
   int part_threads = 128;
   bool dirty = true;
-  int fblocks = 0, pblocks = 0, cblocks = 0;
+  int fgrid = 1;  // CTAs of the fluid pass: one per tile of the work list, rounded up (pool_upload)
+  int pblocks = 0, cblocks = 0;
   int sm_count = 0;
   // Layout of the members (d3q19_options.inplace) while the pool has any; -1
   // when empty.  In place, every member sits at buffer parity 0 between
@@ -1504,7 +1505,7 @@ struct d3q19_pool {
   int inplace = -1;
   double* d_stats = nullptr;  // per-member plane sums and error words (d3q19_pool_mean_stress)
   size_t stats_cap = 0;
-  std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> graphs;  // (steps, fblocks, pblocks, cblocks, inplace)
+  std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> graphs;  // (steps, fgrid, pblocks, cblocks, inplace)
   long long steps = 0;
   // Grid autotuner (d3q19_pool_autotune): on or off, and the advance being
   // timed (its table key, candidate and fluid tile steps), if any.
@@ -1574,7 +1575,6 @@ extern "C" int d3q19_pool_create(int device, int storage, int rebuild_freq, int 
   snprintf(p->dev_name, sizeof(p->dev_name), "%s", pr.name);
   for (char* q = p->dev_name; *q; q++)  // the name is a field of the tuning table's lines
     if (*q == '\t' || *q == '\n' || *q == '|') *q = ' ';
-  p->fblocks = pr.multiProcessorCount * (storage == STORE_F32 ? 5 : 4) * FLUID_CTA_SCALE;
   p->pblocks = pr.multiProcessorCount * 4;
   p->cblocks = pr.multiProcessorCount * 4;
   cudaMemPoolProps mp;
@@ -1725,6 +1725,14 @@ static int pool_upload(d3q19_pool* p) {
   }
   p->nf = (long long)fw.size();
   p->ngr = (long long)pw.size();
+  // Fluid grid: the tile count rounded up to m * 2^k with m in [8, 15] (at
+  // most 1/8 of the CTAs return at once), so that a captured chunk serves
+  // every membership of the same rounded size.
+  {
+    long long g = std::max<long long>(p->nf, 1), unit = 1;
+    while (g > 15 * unit) unit *= 2;
+    p->fgrid = (int)((g + unit - 1) / unit * unit);
+  }
   p->nsph = (long long)cw.size();
   if (threads != p->part_threads) {
     p->part_threads = threads;
@@ -1760,8 +1768,7 @@ static int pool_enqueue(d3q19_pool* p, int nsteps) {
     // In place, the FP32 kernels run 4 blocks/SM: a larger persistent grid
     // would only add a second wave.
     const int aa = p->inplace == 1 ? (par == 0 ? 1 : 2) : 0;
-    const int fb = aa && p->storage == STORE_F32 ? std::min(p->fblocks, 4 * FLUID_CTA_SCALE * p->sm_count) : p->fblocks;
-    POOL_TRY(p, launch_fluid_batch(p->d_fargs, fw, p->d_counts + 0, par, p->storage, aa, fb, p->stream));
+    POOL_TRY(p, launch_fluid_batch(p->d_fargs, fw, p->d_counts + 0, par, p->storage, aa, p->fgrid, p->stream));
     POOL_TRY(p, launch_particle_batch(p->d_pargs, pw, p->d_counts + 1, par, p->part_threads, p->pblocks, p->stream));
     POOL_TRY(p, launch_contact_batch(p->d_pargs, cw, p->d_counts + 2, par, p->cblocks, p->stream));
     if ((j + 1) % p->rebuild == 0)
@@ -1803,13 +1810,11 @@ static std::string tune_key_of(const char* dev_name, int sms, int storage, int i
   return buf;
 }
 
-// The candidates of a pool: fluid 2..4 CTAs per SM (2..5 for the two-buffer
-// FP32 layout, whose register bound admits 5) by particle/contact 1, 2, 4.
-static TuneEntry tune_candidates(const d3q19_pool* p) {
+// The candidates of a pool: particle/contact 1, 2 or 4 CTAs per SM.  The
+// fluid pass runs one CTA per tile (fluid entry 0).
+static TuneEntry tune_candidates(const d3q19_pool*) {
   TuneEntry e;
-  const int fmax = (p->storage == STORE_F32 && p->inplace != 1) ? 5 : 4;
-  for (int f = 2; f <= fmax; f++)
-    for (int q : {1, 2, 4}) e.cand.push_back({f * FLUID_CTA_SCALE, q});
+  for (int q : {1, 2, 4}) e.cand.push_back({0, q});
   e.cost.assign(e.cand.size(), -1.0);
   return e;
 }
@@ -1851,10 +1856,8 @@ static int tune_collect(d3q19_pool* p) {
     }
     if (!all) continue;
     e.best = best;
-    if (it->first == cur) {  // the choice applies from now on
-      p->fblocks = e.cand[best].first * p->sm_count;
+    if (it->first == cur)  // the choice applies from now on
       p->pblocks = p->cblocks = e.cand[best].second * p->sm_count;
-    }
   }
   return 0;
 }
@@ -1895,7 +1898,6 @@ static int tune_choose(d3q19_pool* p, int nsteps, std::string* key_out) {
     for (int i = 0; i < (int)e.cost.size(); i++)
       if (e.cost[i] >= 0 && (c < 0 || e.cost[i] < e.cost[c])) c = i;
   if (c < 0) return -1;
-  p->fblocks = e.cand[c].first * p->sm_count;
   p->pblocks = p->cblocks = e.cand[c].second * p->sm_count;
   if (timed >= 0) *key_out = key;
   return timed;
@@ -1904,7 +1906,7 @@ static int tune_choose(d3q19_pool* p, int nsteps, std::string* key_out) {
 // The graph of a chunk of nsteps at the pool's current grid (captured on
 // first use).
 static int pool_graph(d3q19_pool* p, int nsteps, cudaGraphExec_t* out) {
-  auto key = std::make_tuple(nsteps, p->fblocks, p->pblocks, p->cblocks, p->inplace);
+  auto key = std::make_tuple(nsteps, p->fgrid, p->pblocks, p->cblocks, p->inplace);
   auto it = p->graphs.find(key);
   if (it == p->graphs.end()) {
     cudaGraph_t graph;
@@ -2149,9 +2151,8 @@ extern "C" int d3q19_pool_usage(d3q19_pool* p, size_t* used, size_t* budget, int
 }
 
 extern "C" int d3q19_pool_set_grid(d3q19_pool* p, int fluid_blocks, int particle_blocks, int contact_blocks) {
-  if (!p || fluid_blocks <= 0 || particle_blocks <= 0 || contact_blocks <= 0) return D3Q19_EINVAL;
+  if (!p || fluid_blocks < 0 || particle_blocks <= 0 || contact_blocks <= 0) return D3Q19_EINVAL;
   POOL_LOCK(p);
-  p->fblocks = fluid_blocks;
   p->pblocks = particle_blocks;
   p->cblocks = contact_blocks;
   p->tune = false;
@@ -2178,7 +2179,7 @@ extern "C" int d3q19_pool_tune_state(d3q19_pool* p, int* fluid_per_sm, int* part
   POOL_LOCK(p);
   cudaSetDevice(p->dev);
   if (int rc = tune_collect(p)) return rc;
-  if (fluid_per_sm) *fluid_per_sm = p->fblocks / p->sm_count;
+  if (fluid_per_sm) *fluid_per_sm = 0;  // one CTA per tile
   if (particle_per_sm) *particle_per_sm = p->pblocks / p->sm_count;
   std::lock_guard<std::mutex> lk(g_tune_mu);
   const TuneEntry* e = tune_entry_of(p);
@@ -2254,7 +2255,7 @@ extern "C" int d3q19_tune_import(const char* text) {
     }
     ns = strtod(fld[7].c_str(), &end);
     if (*end || fld[7].empty() || !(ns >= 0)) return D3Q19_EINVAL;
-    if (v[1] > 2 || v[2] > 1 || v[4] < 1 || v[5] < 1) return D3Q19_EINVAL;
+    if (v[1] > 2 || v[2] > 1 || v[5] < 1) return D3Q19_EINVAL;
     TuneEntry e;
     e.cand.push_back({v[4], v[5]});
     e.cost.push_back(ns);
@@ -2275,7 +2276,7 @@ extern "C" int d3q19_tune_clear(void) {
 extern "C" int d3q19_pool_get_grid(d3q19_pool* p, int* fluid_blocks, int* particle_blocks, int* contact_blocks) {
   if (!p) return D3Q19_EINVAL;
   POOL_LOCK(p);
-  if (fluid_blocks) *fluid_blocks = p->fblocks;
+  if (fluid_blocks) *fluid_blocks = p->fgrid;
   if (particle_blocks) *particle_blocks = p->pblocks;
   if (contact_blocks) *contact_blocks = p->cblocks;
   return 0;

@@ -23,9 +23,6 @@ constexpr int TILE_X = 32;
 constexpr int TILE_Y = D3Q19_TILE_Y;
 constexpr int TILE_Z = 4;
 constexpr int FLUID_THREADS = TILE_X * TILE_Y * 2;
-// Fluid CTAs per SM of the pool's persistent grids are counted in units of
-// 256 threads: a lower tile packs more CTAs on an SM.
-constexpr int FLUID_CTA_SCALE = FLUID_THREADS < 256 ? 256 / FLUID_THREADS : 1;
 constexpr int HALO_X = TILE_X + 2;
 constexpr int HALO_Y = TILE_Y + 2;
 constexpr int HALO_Z = TILE_Z + 2;

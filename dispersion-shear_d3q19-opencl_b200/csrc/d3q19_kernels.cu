@@ -214,9 +214,12 @@ __global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4   ? (AA ? FLUID
                                      *reinterpret_cast<SpreadSmem*>(smem_raw));
 }
 
-// The collide-stream pass of many independent lattices in one persistent
-// launch: CTA b takes work items b, b + gridDim.x, ... of the packed list
-// work[k] = {slot, tile} (*nwork items).  slots[2*s + parity] holds lattice
+// The collide-stream pass of many independent lattices in one launch: CTA b
+// takes work item b of the packed list work[k] = {slot, tile} (*nwork items;
+// the grid is at least that long, the CTAs past it return at once).  One CTA
+// per tile lets the hardware schedule the tiles: measured on B200, a served
+// mix of 48 members ran 9,320 MLUPS against 8,296 with a persistent grid of 4
+// CTAs per SM looping over the items, one 150^3 member 6,720 against 6,465.  slots[2*s + parity] holds lattice
 // s's arguments for steps of that buffer parity.  The reference's MRT rates,
 // periodic x/y with z walls, and each lattice's own viscosity law.
 // AA: the pool's layout for this step (every member of a pool shares it and
@@ -234,7 +237,9 @@ __global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? (AA ? FLUID_M
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SpreadSmem& sm = *reinterpret_cast<SpreadSmem*>(smem_raw);
   const int n = *nwork;
-  for (int w = blockIdx.x; w < n; w += gridDim.x) {
+  {
+    const int w = blockIdx.x;
+    if (w >= n) return;
     const int2 it = work[w];
     __shared__ FluidArgs sa;
     {
@@ -249,7 +254,6 @@ __global__ void __launch_bounds__(FLUID_THREADS, sizeof(ST) == 4 ? (AA ? FLUID_M
     const int ntx = a.g.ntx, nty = a.g.nty;
     const int bx = it.y % ntx, by = (it.y / ntx) % nty, bz = it.y / (ntx * nty);
     fluid_tile<0, -1, BC_ZWALL, ST, AA>(a, 0, bx, by, bz, sm);
-    __syncthreads();  // the spread halo is reused by the next item
   }
 }
 

@@ -422,17 +422,20 @@ int d3q19_pool_readmit(d3q19_pool* pool, const int_param_struct* ip, const flp_p
                        const d3q19_options* opt, const void* buf, size_t bytes, int* slot_out);
 /* Budget in use, the budget, and the member count. */
 int d3q19_pool_usage(d3q19_pool* pool, size_t* used, size_t* budget, int* members);
-/* Persistent grid sizes (CTAs) of the batched fluid, particle and contact
- * passes.  Results do not depend on them.  d3q19_pool_set_grid turns the
- * autotuner off. */
+/* Grid sizes (CTAs) of the batched passes.  The fluid pass launches one CTA
+ * per tile of the members (the tile count rounded up to m * 2^k, m in
+ * [8, 15]); d3q19_pool_get_grid reports that grid, and d3q19_pool_set_grid
+ * accepts and ignores a fluid_blocks >= 0.  The particle and contact passes
+ * are persistent grids of the given sizes.  Results do not depend on them.
+ * d3q19_pool_set_grid turns the autotuner off. */
 int d3q19_pool_set_grid(d3q19_pool* pool, int fluid_blocks, int particle_blocks, int contact_blocks);
 int d3q19_pool_get_grid(d3q19_pool* pool, int* fluid_blocks, int* particle_blocks, int* contact_blocks);
 /* Grid autotuner (enable 1 on, 0 off; off when the pool is created).  With
- * it on, d3q19_pool_advance takes the grid from a process-wide table keyed by
- * the device (name and SM count), the pool's storage and layout, and the size
- * class of its work (the bit length of its fluid tile count).  While the
- * class has untried candidates -- fluid 2, 3, 4 CTAs per SM (also 5 for the
- * two-buffer FP32 layout) by particle and contact 1, 2, 4 CTAs per SM -- an
+ * it on, d3q19_pool_advance takes the particle and contact grids from a
+ * process-wide table keyed by the device (name and SM count), the pool's
+ * storage and layout, and the size class of its work (the bit length of its
+ * fluid tile count).  While the class has untried candidates -- 1, 2 or 4
+ * CTAs per SM for the particle and contact passes -- an
  * advance runs them in segments of 100 steps (rounded up to the period; an
  * advance shorter than two segments is one segment, timed when it has at
  * least 100 steps), one candidate per segment, each timed with events on the
@@ -443,9 +446,9 @@ int d3q19_pool_get_grid(d3q19_pool* pool, int* fluid_blocks, int* particle_block
  * process.  Results do not depend on the grid, so the timed segments are
  * ordinary steps of the members. */
 int d3q19_pool_autotune(d3q19_pool* pool, int enable);
-/* The grid in use (CTAs per SM) and the tuner's state for the pool's current
- * work class: settled (0/1), candidates timed, candidates in all.  Waits for
- * a timed advance in flight. */
+/* The grid in use (CTAs per SM; fluid 0: one CTA per tile) and the tuner's
+ * state for the pool's current work class: settled (0/1), candidates timed,
+ * candidates in all.  Waits for a timed advance in flight. */
 int d3q19_pool_tune_state(d3q19_pool* pool, int* fluid_per_sm, int* particle_per_sm, int* settled, int* tried,
                           int* total);
 /* The candidates of the current class with their times (ns per fluid tile
@@ -454,8 +457,8 @@ int d3q19_pool_tune_state(d3q19_pool* pool, int* fluid_per_sm, int* particle_per
 int d3q19_pool_tune_trials(d3q19_pool* pool, int* fluid_per_sm, int* particle_per_sm, double* ns_per_tile_step,
                            int cap, int* n);
 /* The settled classes of the table as text, one line each, tab-separated:
- * device name, SMs, storage, inplace, class, fluid CTAs per SM, particle CTAs
- * per SM, ns per fluid tile step.  *len receives the text's length; the text
+ * device name, SMs, storage, inplace, class, fluid CTAs per SM (0: one CTA per
+ * tile), particle CTAs per SM, ns per fluid tile step.  *len receives the text's length; the text
  * and its NUL are written when cap exceeds it (else ENOMEM, or 0 for cap 0). */
 int d3q19_tune_export(char* buf, size_t cap, size_t* len);
 /* Adds settled classes in d3q19_tune_export's format (a later line of the

@@ -78,7 +78,7 @@ def test_tuning_table_round_trip_without_gpu():
     assert d3.tune_export() == line.replace("\t3\t2\t412.5", "\t4\t1\t400")
     for bad in ("NVIDIA B200\t148\t1\t0\t11\t3\t2\n",          # a field missing
                 "NVIDIA B200\t148\t3\t0\t11\t3\t2\t1.0\n",      # storage out of range
-                "NVIDIA B200\t148\t1\t0\t11\t0\t2\t1.0\n",      # no CTAs
+                "NVIDIA B200\t148\t1\t0\t11\t3\t0\t1.0\n",      # no particle CTAs
                 "NVIDIA B200\t148\t1\t0\t11\t3\t2\tfast\n",     # not a number
                 "\t148\t1\t0\t11\t3\t2\t1.0\n"):                # no device name
         with pytest.raises(d3.D3Q19Error, match="EINVAL"):

@@ -1,4 +1,5 @@
-"""The pool's persistent-grid autotuner (d3q19_pool_autotune) on the GPU.
+"""The pool's grid autotuner (d3q19_pool_autotune) on the GPU: it picks the
+particle and contact grids (the fluid pass runs one CTA per tile).
 
 * Advances of at least 100 steps time the candidates of the pool's work
   class one by one; once all have run, the fastest is kept and used.
@@ -9,6 +10,8 @@
 * The table exported by one process seeds another: an imported class is
   settled at once.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -31,14 +34,14 @@ def test_tuner_settles_on_the_fastest_and_changes_no_result():
     st = pool.tune_state()
     pool.advance(20)  # too short to be timed
     st = pool.tune_state()
-    assert st["tried"] == 0 and not st["settled"] and st["candidates"] == 9
+    assert st["tried"] == 0 and not st["settled"] and st["candidates"] == 3
     n = 20
     while not pool.tune_state()["settled"]:
         pool.advance(100)
         n += 100
-        assert n <= 20 + 100 * 10
+        assert n <= 20 + 100 * 4
     trials = pool.tune_trials()
-    assert len(trials) == 9 and all(t is not None and t > 0 for _, _, t in trials)
+    assert len(trials) == 3 and all(f == 0 and t is not None and t > 0 for f, _, t in trials)
     best = min(trials, key=lambda x: x[2])
     pool.advance(100)  # runs with the choice
     n += 100
@@ -79,18 +82,20 @@ def test_imported_class_is_settled_at_once():
 def test_long_advance_times_one_candidate_per_segment():
     d3.tune_clear()
     pool, slots = pool_with(REQS[:2], True)
-    pool.advance(500)  # five segments of 100 steps, five candidates
+    pool.advance(500)  # three segments of 100 steps time the three candidates; the rest runs at the fastest
     st = pool.tune_state()
-    assert st["tried"] == 5 and not st["settled"]
-    pool.advance(500)  # the other four, then the fastest so far
-    st = pool.tune_state()
-    assert st["settled"] and st["tried"] == st["candidates"] == 9
+    assert st["settled"] and st["tried"] == st["candidates"] == 3
     best = min(pool.tune_trials(), key=lambda x: x[2])
     assert (st["fluid_ctas_per_sm"], st["particle_ctas_per_sm"]) == best[:2]
+    # The fluid pass: one CTA per tile (32 x 4 x 4 tiles from the lattice origin,
+    # buffer layers included), the tile count rounded up by less than 1/8.
+    tiles = sum(math.ceil(r.edge[0] / 32) * math.ceil(r.edge[1] / 4) * math.ceil(r.edge[2] / 4) for r in REQS[:2])
+    fluid_grid = pool.get_grid()[0]
+    assert tiles <= fluid_grid < tiles * 1.125 + 1
     tuned = [state(pool, s) for s in slots]
     pool.close()
     fixed, slots = pool_with(REQS[:2], False)
-    fixed.advance(1000)
+    fixed.advance(500)
     for s, t in zip(slots, tuned):
         bits_equal(t, state(fixed, s))
     fixed.close()
